@@ -1,0 +1,135 @@
+/*
+ * tba.h — C ABI of the B200-native bundle-adjustment library (libtba.so).
+ *
+ * The library replaces the GPU half of TypeCV's `bundleAdjustGpu` operator
+ * (src/sfm/bundle/gpu/bundle.ts:803-839, exported from src/gpu/index.ts:114-118): everything
+ * between the host's packing of the problem and its reading of the result.  The reference host
+ * packs the problem into two arrays (packBundleScene, src/sfm/bundle/gpu/bundle-host.ts:177-218),
+ * uploads them (bundle.ts:267-271), runs its LM/PCG plan of WebGPU dispatches
+ * (bundle.ts:314-772, joint-focal.ts:330-880) and reads one output array back
+ * (bundle.ts:773).  `tba_bundle_adjust` takes exactly those two arrays and fills exactly that
+ * output array, so the reference's host code before and after the call (bundleProblem,
+ * packBundleScene, checkBundleOutput, bundleOutputPose, bundleOutputLandmarks,
+ * bundleOutputReport) stays as it is.
+ *
+ * Conventions: plain pointers and sizes, host memory owned by the caller and only read (inputs)
+ * or written (outputs) during the call; no pointer is kept after return.  Every entry point
+ * returns a tba_status; on failure `tba_last_error` gives the message.  Calls on one device
+ * handle are serialised by the handle; different handles may run concurrently.
+ */
+#ifndef TBA_H
+#define TBA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TBA_ABI_VERSION 1
+
+typedef enum {
+  TBA_OK = 0,
+  /* The problem or the options are invalid (the reference throws RangeError). */
+  TBA_ERROR_ARGUMENT = 1,
+  /* The problem does not fit the device (the reference's "budget" RangeError,
+   * bundle.ts:235-242). */
+  TBA_ERROR_BUDGET = 2,
+  /* A CUDA call failed; the device handle should be closed. */
+  TBA_ERROR_CUDA = 3,
+  /* The library was built without a usable device, or an internal invariant failed. */
+  TBA_ERROR_INTERNAL = 4
+} tba_status;
+
+/* Arithmetic of the solve.  TBA_PRECISION_FP64 is the drop-in (IEEE binary64 throughout).
+ * TBA_PRECISION_MIXED stores the Jacobian factors and runs the Schur product in FP32 with FP64
+ * accumulation, inside an FP64 LM loop (cost, gain, right-hand side and the camera/point block
+ * inverses stay FP64) with one FP64 refinement of each PCG solution.  It has no reference
+ * counterpart. */
+typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
+
+/* TBA_FLAG_TIME_PRODUCTS: bracket every Schur product with CUDA events and report their total
+ * device time in tba_report.product_ms (a few microseconds of host work per PCG iteration). */
+#define TBA_FLAG_TIME_PRODUCTS 1u
+
+/*
+ * The control block of one solve: the reference's `control` uniform
+ * (BundleControl, src/sfm/bundle/gpu/bundle.shade.ts:17-48 and joint-focal.shade.ts:14-42) plus
+ * the host options that its plan consumes (bundle-host.ts:31-113).  Sizes count the trailing
+ * directional points (bearings appended by appendBundleDirections) in `points`.
+ */
+typedef struct {
+  uint32_t cameras;            /* C >= 2 */
+  uint32_t points;             /* P >= 1, including `directional_points` */
+  uint32_t directional_points; /* trailing points that are world bearings */
+  uint32_t observations;       /* M */
+  uint32_t anchor;             /* gauge anchor camera index */
+  uint32_t scale_view;         /* gauge scale camera index */
+  uint32_t iterations;         /* LM iterations, 0..100 (BUNDLE_DEFAULTS.iterations = 20) */
+  uint32_t max_cg;             /* PCG iterations per LM iteration, 1..256 */
+  uint32_t shared_focal;       /* 1: refineSharedFocal (one log-focal unknown, joint-focal.ts) */
+  uint32_t precision;          /* tba_precision */
+  uint32_t flags;              /* TBA_FLAG_* */
+  double huber;                /* Huber threshold in pixels, 1e-12..1e6 */
+  double cg_tolerance;         /* PCG relative residual tolerance, 1e-12..1e-2 */
+  double stall_tolerance;      /* LM stall rule, [0, 1); the device rule is max(this, 1e-9) */
+} tba_control;
+
+/* Timings and traffic of one call, for the operator's `execution` report
+ * (src/geometry/gpu/execution.ts:3-16). */
+typedef struct {
+  double solve_ms;        /* device time from the first kernel to the last (CUDA events) */
+  double upload_ms;       /* device time of the host-to-device copies */
+  double download_ms;     /* device time of the device-to-host copy */
+  double wall_ms;         /* host wall time of the call */
+  double product_ms;      /* device time of the Schur products alone (sampled by events) */
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  uint32_t kernel_launches;
+  uint32_t lm_iterations;  /* LM iterations that ran */
+  uint32_t cg_iterations;  /* PCG iterations that ran (state word 16) */
+  uint32_t product_launches; /* Schur products timed in product_ms */
+  uint32_t engine;         /* 0: grid engine (one problem over the whole GPU) */
+} tba_report;
+
+/* Lengths, in elements, of the arrays of one problem (bundleArraySizes, bundle-host.ts:134-143):
+ * scene = 18C + 3P + 2M doubles, index = 3M + P + 2C + 2 words, and the output of
+ * packBundleResult: 12C + 3P + 26 doubles (+1 with the shared focal: its log scale). */
+size_t tba_scene_size(const tba_control* control);
+size_t tba_index_size(const tba_control* control);
+size_t tba_output_size(const tba_control* control);
+
+typedef struct tba_device tba_device;
+
+/* Open a device handle on CUDA device `ordinal` (replaces ShadeDevice.open,
+ * src/device/gpu/device.ts:240-360).  The handle owns a stream and a workspace that grows to the
+ * largest problem solved and is reused. */
+tba_status tba_device_open(int ordinal, tba_device** device);
+void tba_device_close(tba_device* device);
+/* The message of the last failed call on `device` (or of tba_device_open when device is NULL). */
+const char* tba_last_error(const tba_device* device);
+
+/*
+ * One bundle adjustment: the reference's `bundleAdjustGpuFixed` (bundle.ts:89-800) or, with
+ * control->shared_focal, `bundleAdjustJointFocalGpu` (joint-focal.ts:78-929), from the upload of
+ * the packed arrays to the read of the output array.
+ *
+ * scene:  [poses 12C (R row-major, t) | points 3P | cameras 6C (fx, fy, cx, cy, k1, k2) |
+ *          pixels 2M], observations point-major (packBundleScene).
+ * index:  [obsCamera M | obsPoint M | pointStart P+1 | cameraStart C+1 |
+ *          cameraObservations M | cameraActive C] (bundleIndexLayout, bundle-host.ts:121-131).
+ * output: [poses 12C | points 3P | state 26 (| log focal scale)] (packBundleResult,
+ *          bundle.shade.ts:1115-1125; joint-focal.shade.ts:1119-1129): state word 14 is the
+ *          input error (1: zero gauge baseline, 2: an observation not in front of its camera).
+ * report: may be NULL.
+ */
+tba_status tba_bundle_adjust(tba_device* device, const tba_control* control, const double* scene,
+                             size_t scene_len, const uint32_t* index, size_t index_len,
+                             double* output, size_t output_len, tba_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TBA_H */

@@ -16,7 +16,9 @@
 //      Its output array has the layout of the reference's `packBundleResult`.
 //
 // Both are compiled with -ffp-contract=off and no FMA so that every product and sum rounds the
-// way the reference's JavaScript does.  Parity is pinned by tests/golden (see tests/).
+// way the reference's JavaScript does.  Parity is pinned by tests/golden (see tests/).  The
+// operator's per-point, per-observation and per-camera-row loops run under OpenMP: their
+// iterations are independent, so every value is the same as in a serial run.
 
 #include <algorithm>
 #include <cmath>
@@ -908,6 +910,7 @@ struct Operator {
   }
   // linearizeBundle, bundle.shade.ts:251-297 (joint-focal.shade.ts:266-316).
   void linearize() {
+#pragma omp parallel for schedule(static)
     for (uint32_t i = 0; i < M; i++) {
       const uint32_t c = pb.obs_camera[i], pt = pb.obs_point[i];
       const double* pose = pose_at(c, false);
@@ -953,6 +956,7 @@ struct Operator {
   const double* jf(uint32_t i) const { return &focal[6 * size_t(C) + 6 + 2 * size_t(i)]; }
   // bundlePointBlocks, bundle.shade.ts:378-422 (joint-focal.shade.ts:403-461).
   void point_blocks() {
+#pragma omp parallel for schedule(static)
     for (uint32_t pt = 0; pt < P; pt++) {
       double V[9] = {0}, rhs[3] = {0};
       double* at = &pointb[13 * size_t(pt)];
@@ -1006,6 +1010,7 @@ struct Operator {
   // bundleCameraRows, bundle.shade.ts:497-555, with invertBundleCameraColumns and
   // finalizeBundleCameraInverse, bundle.shade.ts:655-694.
   void camera_rows() {
+#pragma omp parallel for schedule(dynamic, 1)
     for (uint32_t c = 0; c < C; c++)
       for (int j = 0; j < 6; j++) {
         double aRow[6] = {0}, sRow[6] = {0}, rhs = 0;
@@ -1040,6 +1045,7 @@ struct Operator {
         }
         camRhs[6 * size_t(c) + j] = rhs;
       }
+#pragma omp parallel for schedule(static)
     for (uint32_t c = 0; c < C; c++) {
       double* inv = &camInv[36 * size_t(c)];
       for (int column = 0; column < 6; column++) {
@@ -1070,6 +1076,7 @@ struct Operator {
   // joint-focal.shade.ts:1138-1205.
   void focal_terms() {
     const size_t n = 6 * size_t(C);
+#pragma omp parallel for schedule(dynamic, 1)
     for (uint32_t c = 0; c < C; c++)
       for (int j = 0; j < 6; j++) {
         double value = 0;
@@ -1167,6 +1174,7 @@ struct Operator {
   // bundleSchurPoint + bundleSchurCamera (rows), bundle.shade.ts:185-225,
   // joint-focal.shade.ts:197-253.
   void schur_product() {
+#pragma omp parallel for schedule(static)
     for (uint32_t pt = 0; pt < P; pt++) {
       const double* at = &pointb[13 * size_t(pt)];
       double rhs[3] = {0, 0, 0};
@@ -1184,6 +1192,7 @@ struct Operator {
         y()[3 * size_t(pt) + j] = v;
       }
     }
+#pragma omp parallel for schedule(dynamic, 6)
     for (uint32_t row = 0; row < 6 * C; row++) {
       const uint32_t c = row / 6, j = row % 6;
       const double* A = &camA[36 * size_t(c)];
@@ -1264,6 +1273,7 @@ struct Operator {
       else std::memcpy(moved, p_, sizeof moved);
       std::memcpy(&trial_pose[12 * size_t(c)], moved, sizeof moved);
     }
+#pragma omp parallel for schedule(static)
     for (uint32_t pt = 0; pt < P; pt++) {
       const double* at = &pointb[13 * size_t(pt)];
       double rhs[3] = {at[9], at[10], at[11]};

@@ -48,7 +48,7 @@ def build(force: bool = False) -> str:
     if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(SOURCE):
         os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
         tmp = LIB_PATH + f".{os.getpid()}.tmp"
-        subprocess.check_call(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared",
+        subprocess.check_call(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared",
                                "-o", tmp, SOURCE])
         os.replace(tmp, LIB_PATH)
     return LIB_PATH

@@ -1,0 +1,220 @@
+"""Parity of the CUDA operator (libtba.so, through its C ABI) with the oracle.
+
+* the reference's recorded GPU results on its own fixtures (tests/golden/reference_records.json);
+* the reference GPU operator's algorithm restated on the CPU (oracle.gpu_operator), same inputs;
+* the reference's CPU bundle adjustment (oracle.cpu_bundle_adjust, exact dense solve) at a tight
+  PCG tolerance: final robust cost within 1e-9 relative and RMS within 1e-6 px;
+* the reference's own test assertions (tests/typeshade/cpu.test.mjs, focal.test.mjs) on the
+  GPU result, and edge cases: zero iterations, rejected solves, windows, bearings, long tracks.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import typecv_b200 as tb
+from typecv_b200 import synthetic as S
+from oracle import bundle_adjust as ob
+from reference_cases import bundle_fixture, bundle_metrics, joint_focal_fixture, skew_bundle_fixture
+
+pytestmark = pytest.mark.gpu
+
+RECORDS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_records.json")))["records"]
+COST_REL = 1e-9   # final robust cost, FP64 form
+RMS_PX = 1e-6     # reprojection RMS, FP64 form
+
+
+@pytest.fixture(scope="module")
+def device():
+    dev = tb.ShadeDevice.open(0)
+    yield dev
+    dev.close()
+
+
+def record_fixture(rec):
+    f = rec["fixture"]
+    return skew_bundle_fixture(f["views"], f["count"]) if f["skew"] else bundle_fixture(views=f["views"], count=f["count"])
+
+
+@pytest.mark.parametrize("rec", RECORDS, ids=lambda r: r["name"] + "/" + str(r["options"]["iterations"]))
+def test_reproduces_reference_gpu_records(device, rec):
+    out = tb.bundle_adjust_gpu(device, record_fixture(rec), rec["options"])
+    serial = rec["variants"][0]
+    costs = [v["finalCost"] for v in rec["variants"]]
+    cg = [v["cgIterations"] for v in rec["variants"]]
+    final = out["diagnostics"]["finalCost"]
+    assert abs(final - serial["finalCost"]) <= COST_REL * serial["finalCost"], (final, serial)
+    assert min(costs) * (1 - 1e-10) <= final <= max(costs) * (1 + 1e-10)
+    assert min(cg) - 2 <= out["cgIterations"] <= max(cg) + 2
+    assert out["linearSolverFailures"] == 0
+
+
+def _compare_operator(device, model, options, pose_tol=1e-7):
+    got = tb.bundle_adjust_gpu(device, model, options)
+    want = ob.gpu_operator(model, options)
+    gd, wd = got["diagnostics"], want["diagnostics"]
+    assert abs(gd["initialCost"] - wd["initialCost"]) <= 1e-12 * wd["initialCost"]
+    assert abs(gd["finalCost"] - wd["finalCost"]) <= COST_REL * max(wd["finalCost"], 1e-300) + 1e-18
+    assert abs(gd["finalRmsePx"] - wd["finalRmsePx"]) <= RMS_PX
+    assert gd["acceptedSteps"] == wd["acceptedSteps"] and gd["rejectedSteps"] == wd["rejectedSteps"]
+    for a, b in zip(got["reconstruction"]["views"], want["reconstruction"]["views"]):
+        assert np.max(np.abs(np.asarray(a["pose"]["t"]) - b["pose"]["t"])) < pose_tol
+        assert np.max(np.abs(np.asarray(a["pose"]["R"]) - b["pose"]["R"])) < pose_tol
+        assert abs(a["camera"]["fx"] - b["camera"]["fx"]) <= 1e-9 * b["camera"]["fx"]
+    return got, want
+
+
+@pytest.mark.parametrize("options", [
+    {"iterations": 15, "huberPx": 1},
+    {"iterations": 15, "huberPx": 1, "refineSharedFocal": True},
+    {"iterations": 10, "variableViewIds": [30, 40]},
+    {"iterations": 5, "variableViewIds": []},
+    {"iterations": 12, "cgRelativeTolerance": 1e-10, "maxCgIterations": 200, "stallTolerance": 1e-4},
+])
+def test_matches_operator_oracle_on_reference_fixture(device, options):
+    for settings in ({}, {"outlier": True}, {"shift": (7, -3, 2)}):
+        model = bundle_fixture(**settings)
+        opts = dict(options)
+        if "shift" in settings and "variableViewIds" not in opts:
+            opts.update(anchorViewId=20, scaleViewId=40)
+        _compare_operator(device, model, opts)
+
+
+def test_cpu_tier_assertions(device):
+    # tests/typeshade/cpu.test.mjs:533-607 on the CUDA operator.
+    for settings in ({}, {"outlier": True}, {"shift": (7, -3, 2)}):
+        inp = bundle_fixture(**settings)
+        snapshot = json.dumps([list(map(float, p["xyz"])) for p in inp["landmarks"]])
+        initial = bundle_metrics(inp, 1)
+        shifted = "shift" in settings
+        anchor, scale_view = (1, 3) if shifted else (0, 1)
+        r = tb.bundle_adjust_gpu(device, inp, {"iterations": 15, "huberPx": 1,
+                                               **({"anchorViewId": 20, "scaleViewId": 40} if shifted else {})})
+        actual = bundle_metrics(r["reconstruction"], 1)
+        assert r["diagnostics"]["acceptedSteps"] > 0
+        assert actual["cost"] < initial["cost"] * 0.05
+        assert abs(actual["cost"] - r["diagnostics"]["finalCost"]) < 1e-6
+        assert json.dumps([list(map(float, p["xyz"])) for p in inp["landmarks"]]) == snapshot
+        v = r["reconstruction"]["views"][anchor]["pose"]
+        assert np.array_equal(v["R"], inp["views"][anchor]["pose"]["R"]) and np.array_equal(v["t"], inp["views"][anchor]["pose"]["t"])
+        a = ob.camera_center(r["reconstruction"]["views"][anchor]["pose"])
+        b = ob.camera_center(r["reconstruction"]["views"][scale_view]["pose"])
+        assert abs(np.linalg.norm(a - b) - r["diagnostics"]["baseline"]) < 1e-9
+        assert actual["observations"] == 160
+        assert r["execution"]["cpuStages"] == []
+    inp = bundle_fixture()
+    local = tb.bundle_adjust_gpu(device, inp, {"iterations": 10, "variableViewIds": [30, 40]})
+    assert local["diagnostics"]["finalCost"] < local["diagnostics"]["initialCost"]
+    for i in (0, 1):
+        assert np.array_equal(local["reconstruction"]["views"][i]["pose"]["t"], inp["views"][i]["pose"]["t"])
+    unchanged = tb.bundle_adjust_gpu(device, inp, {"iterations": 0})
+    for a, b in zip(unchanged["reconstruction"]["landmarks"], inp["landmarks"]):
+        assert np.array_equal(a["xyz"], b["xyz"])
+    points_only = tb.bundle_adjust_gpu(device, inp, {"iterations": 5, "variableViewIds": []})
+    assert points_only["diagnostics"]["finalCost"] < points_only["diagnostics"]["initialCost"]
+    for a, b in zip(points_only["reconstruction"]["views"], inp["views"]):
+        assert np.array_equal(a["pose"]["t"], b["pose"]["t"])
+    rejected = tb.bundle_adjust_gpu(device, inp, {"iterations": 1, "maxCgIterations": 1, "cgRelativeTolerance": 1e-12})
+    assert rejected["diagnostics"]["acceptedSteps"] == 0 and rejected["linearSolverFailures"] > 0
+    for a, b in zip(rejected["reconstruction"]["landmarks"], inp["landmarks"]):
+        assert np.array_equal(a["xyz"], b["xyz"])
+    zero = {**inp, "views": [{**v, "pose": inp["views"][0]["pose"]} if i == 1 else v for i, v in enumerate(inp["views"])]}
+    with pytest.raises(tb.RangeError, match="baseline"):
+        tb.bundle_adjust_gpu(device, zero, {"iterations": 0})
+    behind = {**inp, "landmarks": [{**p, "xyz": np.array([0.0, 0, -5])} if i == 0 else p for i, p in enumerate(inp["landmarks"])]}
+    with pytest.raises(tb.RangeError, match="in front"):
+        tb.bundle_adjust_gpu(device, behind, {"iterations": 0})
+
+
+FOCAL = {"iterations": 40, "refineSharedFocal": True, "maxCgIterations": 256, "cgRelativeTolerance": 1e-10}
+
+
+def test_joint_focal_recovers_truth_and_matches_cpu_reference(device):
+    # tests/typeshade/focal.test.mjs:13-45
+    jf = joint_focal_fixture()
+    inp, truth = jf["input"], jf["truth"]
+    expected = ob.cpu_bundle_adjust(inp, FOCAL)
+    actual = tb.bundle_adjust_gpu(device, inp, FOCAL)
+    d = actual["diagnostics"]
+    assert d["finalCost"] < 1e-7 and d["finalRmsePx"] < 1e-4 and d["initialCost"] > 50000
+    views = actual["reconstruction"]["views"]
+    scale = views[0]["camera"]["fx"] / inp["views"][0]["camera"]["fx"]
+    assert abs(views[0]["camera"]["fx"] - truth["views"][0]["camera"]["fx"]) < 0.001
+    for v, v0 in zip(views, inp["views"]):
+        assert abs(v["camera"]["fx"] / v0["camera"]["fx"] - scale) < 1e-12
+        assert abs(v["camera"]["fy"] / v0["camera"]["fy"] - scale) < 1e-12
+        assert v["camera"]["k1"] == v0["camera"]["k1"] and v["camera"]["k2"] == v0["camera"]["k2"]
+    assert np.array_equal(views[0]["pose"]["R"], inp["views"][0]["pose"]["R"])
+    assert abs(actual["diagnostics"]["finalCost"] - expected["diagnostics"]["finalCost"]) < 1e-7
+
+
+def test_joint_focal_zero_iterations_and_fixed_poses(device):
+    # tests/typeshade/focal.test.mjs:47-71
+    inp = joint_focal_fixture(points=20, views=4)["input"]
+    zero = tb.bundle_adjust_gpu(device, inp, {**FOCAL, "iterations": 0})
+    assert zero["diagnostics"]["finalCost"] == zero["diagnostics"]["initialCost"]
+    assert zero["diagnostics"]["acceptedSteps"] == 0
+    for a, b in zip(zero["reconstruction"]["views"], inp["views"]):
+        assert a["camera"] == b["camera"] and np.array_equal(a["pose"]["R"], b["pose"]["R"])
+    local = tb.bundle_adjust_gpu(device, inp, {**FOCAL, "iterations": 15, "variableViewIds": []})
+    assert local["diagnostics"]["finalCost"] < local["diagnostics"]["initialCost"]
+    for a, b in zip(local["reconstruction"]["views"], inp["views"]):
+        assert np.array_equal(a["pose"]["t"], b["pose"]["t"])
+    assert local["reconstruction"]["views"][0]["camera"]["fx"] > inp["views"][0]["camera"]["fx"]
+
+
+@pytest.mark.parametrize("shared", [True, False])
+def test_synthetic_ring_matches_cpu_reference(device, shared):
+    # Configuration 0 (10 cameras / 2,000 points), tight PCG: the exact dense CPU solve.
+    scene = S.ring_scene()
+    rec = scene.as_reconstruction()
+    opts = {"iterations": 20, "huberPx": 2.0, "refineSharedFocal": shared, "cgRelativeTolerance": 1e-12,
+            "maxCgIterations": 256}
+    got = tb.bundle_adjust_gpu(device, rec, opts)
+    want = ob.cpu_bundle_adjust(rec, opts)
+    gd, wd = got["diagnostics"], want["diagnostics"]
+    assert abs(gd["finalCost"] - wd["finalCost"]) <= COST_REL * wd["finalCost"], (gd, wd)
+    assert abs(gd["finalRmsePx"] - wd["finalRmsePx"]) <= RMS_PX
+    # 3% uniform outliers keep the Huber cost high; the inliers converge.
+    assert gd["finalCost"] < gd["initialCost"] and gd["acceptedSteps"] > 0
+
+
+def test_long_tracks_and_skewed_cameras(device):
+    # Points seen by more than 32 cameras take the multi-round warp path.
+    scene = S.ring_scene(seed=3, cameras=40, points=200)
+    assert np.bincount(scene.obs_point).max() > 32
+    rec = scene.as_reconstruction()
+    for shared in (False, True):
+        _compare_operator(device, rec, {"iterations": 6, "refineSharedFocal": shared}, pose_tol=1e-6)
+    _compare_operator(device, skew_bundle_fixture(17, 512), {"iterations": 3, "maxCgIterations": 96})
+
+
+def test_directional_constraints(device):
+    inp = bundle_fixture()
+    direction = {"trackId": 1000, "direction": np.array([0.1, 0.05, 1.0]),
+                 "observations": [{"viewId": 10, "featureId": 500, "pixel": [560.0, 300.0]},
+                                  {"viewId": 20, "featureId": 500, "pixel": [548.0, 301.0]}]}
+    opts = {"iterations": 8, "directionalConstraints": [direction]}
+    got = tb.bundle_adjust_gpu(device, inp, opts)
+    want = ob.gpu_operator(inp, opts)
+    assert abs(got["diagnostics"]["finalCost"] - want["diagnostics"]["finalCost"]) <= COST_REL * want["diagnostics"]["finalCost"]
+    d = got["directionalConstraints"][0]["direction"]
+    assert abs(np.linalg.norm(d) - 1) < 1e-12
+    assert np.max(np.abs(d - want["directionalConstraints"][0]["direction"])) < 1e-7
+    assert got["diagnostics"]["pointParameters"] == 3 * 40 + 2
+
+
+def test_helix_midsize_matches_operator_oracle(device):
+    scene = S.helix_scene(cameras=40, points=4000)
+    s, i = scene.packed()
+    for shared in (True, False):
+        ctl = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, iterations=6, shared_focal=shared)
+        out, rep = tb.solve_packed(device, ctl, s, i)
+        packed = {"C": scene.C, "P": scene.P, "M": scene.M, "scene": s, "index": i}
+        ref = ob.gpu_operator_packed(packed, 0, 1, iterations=6, huber=2.0, max_cg=ctl.max_cg, shared=shared)
+        base = 12 * scene.C + 3 * scene.P
+        assert abs(out[base + 6] - ref[base + 6]) <= COST_REL * ref[base + 6]
+        assert abs(out[base + 16] - ref[base + 16]) <= 2 * 6
+        assert rep["lm_iterations"] >= 1

@@ -1,0 +1,90 @@
+"""ctypes binding of libtba.so (include/tba.h).
+
+The library is loaded from this package's directory only.  There is no fallback: when the
+library is missing or fails to load, every entry point raises ``LibraryError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtba.so")
+
+TBA_OK, TBA_ERROR_ARGUMENT, TBA_ERROR_BUDGET, TBA_ERROR_CUDA, TBA_ERROR_INTERNAL = range(5)
+TBA_PRECISION_FP64, TBA_PRECISION_MIXED = 0, 1
+TBA_FLAG_TIME_PRODUCTS = 1
+
+# Every symbol include/tba.h declares.
+EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
+           "tba_last_error", "tba_bundle_adjust")
+
+
+class LibraryError(RuntimeError):
+    """libtba.so is missing or unusable: the operator has no other implementation."""
+
+
+class Control(ctypes.Structure):
+    _fields_ = [
+        ("cameras", ctypes.c_uint32), ("points", ctypes.c_uint32),
+        ("directional_points", ctypes.c_uint32), ("observations", ctypes.c_uint32),
+        ("anchor", ctypes.c_uint32), ("scale_view", ctypes.c_uint32),
+        ("iterations", ctypes.c_uint32), ("max_cg", ctypes.c_uint32),
+        ("shared_focal", ctypes.c_uint32), ("precision", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+        ("huber", ctypes.c_double), ("cg_tolerance", ctypes.c_double), ("stall_tolerance", ctypes.c_double),
+    ]
+
+
+class Report(ctypes.Structure):
+    _fields_ = [
+        ("solve_ms", ctypes.c_double), ("upload_ms", ctypes.c_double), ("download_ms", ctypes.c_double),
+        ("wall_ms", ctypes.c_double), ("product_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint32), ("lm_iterations", ctypes.c_uint32),
+        ("cg_iterations", ctypes.c_uint32), ("product_launches", ctypes.c_uint32), ("engine", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise LibraryError(f"libtba.so is not built ({path}); run `python -m typecv_b200.build`")
+    try:
+        lib = ctypes.CDLL(path)
+    except OSError as e:
+        raise LibraryError(f"libtba.so failed to load: {e}") from e
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    lib.tba_scene_size.restype = ctypes.c_size_t
+    lib.tba_scene_size.argtypes = [P(Control)]
+    lib.tba_index_size.restype = ctypes.c_size_t
+    lib.tba_index_size.argtypes = [P(Control)]
+    lib.tba_output_size.restype = ctypes.c_size_t
+    lib.tba_output_size.argtypes = [P(Control)]
+    lib.tba_device_open.restype = ctypes.c_int
+    lib.tba_device_open.argtypes = [ctypes.c_int, P(vp)]
+    lib.tba_device_close.restype = None
+    lib.tba_device_close.argtypes = [vp]
+    lib.tba_last_error.restype = ctypes.c_char_p
+    lib.tba_last_error.argtypes = [vp]
+    lib.tba_bundle_adjust.restype = ctypes.c_int
+    lib.tba_bundle_adjust.argtypes = [vp, P(Control), P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_uint32),
+                                      ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t, P(Report)]
+    _lib = lib
+    return lib
+
+
+def dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def uptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
