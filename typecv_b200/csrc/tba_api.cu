@@ -323,7 +323,10 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   CUDA_TRY(cudaEventRecord(e_up, s));
 
   uint32_t launches = 0, lm_done = 0;
+  // Event pairs around the Schur products; after the solve, only the products that ran PCG steps
+  // (the first `steps` of each LM iteration; later ones are guarded no-ops) count.
   std::vector<std::pair<size_t, size_t>> product_events;
+  std::vector<std::pair<size_t, uint32_t>> product_spans;  // (first event pair, real steps) per LM iteration
   const bool time_products = (ctl->flags & TBA_FLAG_TIME_PRODUCTS) != 0;
   tba::launch_initialize(p, s);
   tba::launch_cost(p, s);
@@ -332,6 +335,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   CUDA_TRY(cudaGetLastError());
   bool lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
+    const size_t first_pair = product_events.size();
     tba::launch_point_pass(p, s);
     tba::launch_camera_pass(p, s);
     tba::launch_camera_finish(p, s);
@@ -365,7 +369,10 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     launches += 4;
     CUDA_TRY(cudaGetLastError());
     lm_done++;
-    lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
+    CUDA_TRY(cudaMemcpyAsync(d->pinned, p.state, 32 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    lm_active = d->pinned[tba::S_ACTIVE] != 0;
+    product_spans.emplace_back(first_pair, uint32_t(d->pinned[tba::S_CG_SOLVE_STEPS]));
   }
   tba::launch_pack(p, s);
   launches++;
@@ -385,12 +392,18 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     CUDA_TRY(cudaEventElapsedTime(&ms, e_solved, e_down));
     report->download_ms = ms;
     double total = 0;
-    for (auto& pe : product_events) {
-      CUDA_TRY(cudaEventElapsedTime(&ms, d->events[pe.first], d->events[pe.second]));
-      total += ms;
+    uint32_t counted = 0;
+    for (size_t k = 0; k < product_spans.size(); k++) {
+      const size_t end = k + 1 < product_spans.size() ? product_spans[k + 1].first : product_events.size();
+      const size_t last = std::min(end, product_spans[k].first + product_spans[k].second);
+      for (size_t j = product_spans[k].first; j < last; j++) {
+        CUDA_TRY(cudaEventElapsedTime(&ms, d->events[product_events[j].first], d->events[product_events[j].second]));
+        total += ms;
+        counted++;
+      }
     }
     report->product_ms = total;
-    report->product_launches = uint32_t(product_events.size());
+    report->product_launches = counted;
     report->h2d_bytes = h2d;
     report->d2h_bytes = out_len * sizeof(double);
     report->kernel_launches = launches;
