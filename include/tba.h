@@ -128,6 +128,35 @@ tba_status tba_bundle_adjust(tba_device* device, const tba_control* control, con
                              size_t scene_len, const uint32_t* index, size_t index_len,
                              double* output, size_t output_len, tba_report* report);
 
+/*
+ * The robust cost of a packed scene that is already in device memory, computed without
+ * allocating.  No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc — applications whose device memory belongs to their own allocator (a caching pool
+ * or an arena reserved at start-up, where a library allocation fails at the limit or fragments
+ * it) and code on latency-critical threads (cudaMalloc and cudaFree can synchronise the device).
+ *
+ * scene, index: device pointers to the packed arrays of tba_bundle_adjust (same layouts; only the
+ *   poses, points, cameras, pixels and the obsCamera/obsPoint sections are read).  Indices are not
+ *   trusted: an out-of-range one is skipped and counted.
+ * result: device pointer to 4 doubles: robust cost (Huber, control->huber), sum of squared
+ *   errors, observations whose projection failed (behind the camera or outside the lens model),
+ *   observations with an out-of-range index.  With the same inputs this equals the initial cost
+ *   and squared error of tba_bundle_adjust (state words 8 and 9; word 24 is sqrt(SSE / M)).
+ * stream: the cudaStream_t to run on (NULL: the default stream).  The call is asynchronous: the
+ *   result is ready when the stream reaches it.
+ * message: optional buffer for the error text.
+ *
+ * Limit: at most 16,777,216 observations (4,096 tiles of 4,096); larger scenes are refused with
+ * TBA_ERROR_ARGUMENT.  The tile partials live in one fixed 128 KiB array that every GPU loading
+ * the library holds until exit.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the caller's current device; make that first call before any stream
+ * capture.  Every call shares the array: each call writes every tile row it reads, so nothing has
+ * to start at zero, but calls that overlap on the GPU (different streams, not ordered) race and
+ * must be serialised by the caller.
+ */
+tba_status tba_scene_cost_noalloc(const tba_control* control, const double* scene, const uint32_t* index,
+                                  double* result, void* stream, char* message, size_t message_len);
+
 #ifdef __cplusplus
 }
 #endif

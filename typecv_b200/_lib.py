@@ -17,7 +17,7 @@ TBA_FLAG_TIME_PRODUCTS = 1
 
 # Every symbol include/tba.h declares.
 EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
-           "tba_last_error", "tba_bundle_adjust")
+           "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc")
 
 
 class LibraryError(RuntimeError):
@@ -78,6 +78,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tba_bundle_adjust.restype = ctypes.c_int
     lib.tba_bundle_adjust.argtypes = [vp, P(Control), P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_uint32),
                                       ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t, P(Report)]
+    lib.tba_scene_cost_noalloc.restype = ctypes.c_int
+    lib.tba_scene_cost_noalloc.argtypes = [P(Control), vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t]
     _lib = lib
     return lib
 
