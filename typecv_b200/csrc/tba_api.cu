@@ -355,7 +355,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
           tba::launch_product(p, s);
         }
         tba::launch_product_finish(p, s);
-        launches += 2;
+        launches += 4;
       }
       CUDA_TRY(cudaGetLastError());
       done += k;

@@ -44,6 +44,8 @@ enum StateWord : int {
   S_FOCAL_INV = 29,        // 1 / S_ff (preconditioner), -1 when not positive
   S_FOCAL_RHS = 30,        // reduced focal right-hand side
   S_POINT_FAILED = 31,     // a point block failed this LM iteration
+  S_ALPHA = 32,            // step length of the current PCG iteration
+  S_BETA = 33,             // direction update of the current PCG iteration
   S_WORDS = 64
 };
 
@@ -116,13 +118,16 @@ void launch_camera_pass(const Params& p, cudaStream_t s);
 void launch_camera_finish(const Params& p, cudaStream_t s);
 void launch_pcg_init(const Params& p, cudaStream_t s);
 void launch_product(const Params& p, cudaStream_t s);
+// One PCG step after the product: column reduction of the product partials and alpha, the
+// distributed update of x, r, z and beta, then the new direction p.
 void launch_product_finish(const Params& p, cudaStream_t s);
 void launch_update_cameras(const Params& p, cudaStream_t s);
 void launch_update_points(const Params& p, cudaStream_t s);
 void launch_accept(const Params& p, cudaStream_t s);
 void launch_commit(const Params& p, cudaStream_t s);
 void launch_pack(const Params& p, cudaStream_t s);
-// Blocks of the product-finish kernel, and the dynamic shared memory of the product kernel.
+// Blocks of the widest finish kernel (sizes blk_part), and the dynamic shared memory of the
+// product kernel.
 uint32_t product_finish_blocks(const Params& p);
 size_t product_smem_bytes(const Params& p);
 // Largest unknown count whose accumulators fit one block's shared memory.

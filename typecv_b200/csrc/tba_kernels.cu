@@ -26,6 +26,22 @@
 
 #include "tba_engine.cuh"
 
+// Compile-time tuning of the heavy kernels (occupancy floors of __launch_bounds__, and whether
+// the Schur product keeps a lane's W block in registers between its two uses or re-reads it
+// from L1 for the scatter).
+#ifndef TBA_PRODUCT_MIN_BLOCKS
+#define TBA_PRODUCT_MIN_BLOCKS 2
+#endif
+#ifndef TBA_PRODUCT_RELOAD
+#define TBA_PRODUCT_RELOAD 1
+#endif
+#ifndef TBA_POINT_MIN_BLOCKS
+#define TBA_POINT_MIN_BLOCKS 2
+#endif
+#ifndef TBA_CAMERA_MIN_BLOCKS
+#define TBA_CAMERA_MIN_BLOCKS 3
+#endif
+
 namespace tba {
 namespace {
 
@@ -129,7 +145,7 @@ __global__ void k_initialize(Params P) {
     st[S_INPUT_ERROR] = 1;
     st[S_ACTIVE] = 0;
   }
-  *P.ticket = 0;
+  for (int k = 0; k < 8; k++) P.ticket[k] = 0;
 }
 
 // ---- K3/K4: the linearised cost of the scene ---------------------------------------------------
@@ -264,7 +280,7 @@ __device__ inline void point_finish(const Params& P, uint32_t pt, const double (
 }
 
 template <bool SHARED>
-__global__ void __launch_bounds__(kPointThreads) k_point_pass(Params P) {
+__global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_pass(Params P) {
   __shared__ double red[kScalarPartials * (kPointThreads / 32)];
   if (P.state[S_ACTIVE] == 0) return;
   const double lambda = P.state[S_LAMBDA], logf = P.state[S_LOG_FOCAL];
@@ -308,7 +324,7 @@ __global__ void __launch_bounds__(kPointThreads) k_point_pass(Params P) {
 
 // ---- K6/K8/K21: camera blocks ------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kCameraThreads) k_camera_pass(Params P) {
+__global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_camera_pass(Params P) {
   __shared__ double red[kCameraPartials * (kCameraThreads / 32)];
   if (P.state[S_ACTIVE] == 0) return;
   const uint32_t ch = blockIdx.x, c = P.chunk_cam[ch];
@@ -490,7 +506,7 @@ __global__ void __launch_bounds__(1024) k_pcg_init(Params P) {
 // ---- K10/K11: the Schur product S p, one pass over W -------------------------------------------
 
 template <bool SHARED>
-__global__ void __launch_bounds__(kProductThreads, 1) k_product(Params P) {
+__global__ void __launch_bounds__(kProductThreads, TBA_PRODUCT_MIN_BLOCKS) k_product(Params P) {
   extern __shared__ double acc[];
   if (P.state[S_CG_ACTIVE] == 0) return;
   const uint32_t m = P.m;
@@ -547,6 +563,10 @@ __global__ void __launch_bounds__(kProductThreads, 1) k_product(Params P) {
       for (int j = 0; j < 3; j++) y[j] = __shfl_sync(kFull, y[j], tail);
       if (valid) {
         double* ac = acc + 6 * size_t(c);
+        if (TBA_PRODUCT_RELOAD) {
+#pragma unroll
+          for (int k = 0; k < WD; k++) w[k] = __ldg(P.W + k * M + i);
+        }
 #pragma unroll
         for (int k = 0; k < 6; k++) atomicAdd(ac + k, -(w[k * 3] * y[0] + w[k * 3 + 1] * y[1] + w[k * 3 + 2] * y[2]));
         if (SHARED) ef += w[18] * y[0] + w[19] * y[1] + w[20] * y[2];
@@ -597,125 +617,166 @@ __global__ void __launch_bounds__(kProductThreads, 1) k_product(Params P) {
   for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) out[j] = acc[j];
 }
 
-// ---- K12: reduce the product partials, then (last block) one PCG step ---------------------------
+// ---- K12: one PCG step, in three short kernels --------------------------------------------------
+//
+// k_product_reduce   column-parallel sum of the product blocks' partial rows (fixed order), the
+//                    camera rows of S p = U_c p_c + H_cf p_f - sum, their p . Sp share; its last
+//                    block adds the focal row and forms alpha = rho / p.Sp (with the reference's
+//                    breakdown checks).
+// k_pcg_update       x += alpha p, r -= alpha Sp, z = M^-1 r by camera blocks (252 rows per block,
+//                    so no camera straddles two blocks); its last block forms the residual, rho,
+//                    the convergence test and beta.
+// k_pcg_direction    p = z + beta p.
 
-constexpr int kFinishThreads = 256;
+constexpr int kReduceThreads = 256;  // 8 warps; 32 columns per block
+constexpr int kUpdateRows = 252;     // 42 cameras per block
+constexpr int kUpdateThreads = 256;
 
-__device__ void pcg_advance(const Params& P, double den, double* red) {
-  double* st = P.state;
-  __shared__ int stop;
-  if (threadIdx.x == 0) {
-    stop = 0;
-    if (!(den > 0)) {
-      st[S_CG_ACTIVE] = 0;
-      st[S_CG_FAILED] = 1;
-      stop = 1;
-    } else if (!(fabs(st[S_RHO] / den) < 1e20)) {
-      st[S_CG_ACTIVE] = 0;
-      st[S_CG_FAILED] = 1;
-      stop = 1;
-    }
-  }
+// True in the block that finishes last.  Every thread fences its own writes before the barrier,
+// so the last block sees every block's results (read them with __ldcg).
+__device__ inline bool last_block(uint32_t* ticket) {
+  __shared__ bool last;
+  __threadfence();
   __syncthreads();
-  if (stop) return;
-  const double alpha = st[S_RHO] / den;
-  double v[2] = {0, 0};
-  for (uint32_t i = threadIdx.x; i < P.m; i += blockDim.x) {
-    P.x[i] += alpha * P.p[i];
-    const double rr = P.r[i] - alpha * __ldcg(P.Sp + i);
-    P.r[i] = rr;
-    v[0] += rr * rr;
-  }
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < P.m; i += blockDim.x) {
-    const double zz = precondition(P, i);
-    P.z[i] = zz;
-    v[1] += zz * P.r[i];
-  }
-  block_sum(v, red);
-  if (threadIdx.x == 0) {
-    const double residual = v[0], rho = v[1];
-    st[S_CG_STEPS] += 1;
-    st[S_CG_SOLVE_STEPS] += 1;
-    st[S_R2] = residual;
-    stop = 0;
-    if (residual <= P.tol * P.tol * st[S_R0]) {
-      st[S_CG_ACTIVE] = 0;
-      st[S_CG_CONVERGED] = 1;
-      stop = 1;
-    } else if (!(rho > 0)) {
-      st[S_CG_ACTIVE] = 0;
-      st[S_CG_FAILED] = 1;
-      stop = 1;
-    } else {
-      red[0] = rho / st[S_RHO];
-      st[S_RHO] = rho;
-    }
-  }
-  __syncthreads();
-  if (stop) return;
-  const double beta = red[0];
-  for (uint32_t i = threadIdx.x; i < P.m; i += blockDim.x) P.p[i] = P.z[i] + beta * P.p[i];
+  if (last) __threadfence();
+  return last;
 }
 
 template <bool SHARED>
-__global__ void __launch_bounds__(kFinishThreads) k_product_finish(Params P) {
-  __shared__ double red[2 * (kFinishThreads / 32)];
-  __shared__ bool last;
+__global__ void __launch_bounds__(kReduceThreads) k_product_reduce(Params P) {
+  __shared__ double part[8][33];
+  __shared__ double red[2 * (kReduceThreads / 32)];
   if (P.state[S_CG_ACTIVE] == 0) return;
-  const uint32_t n = 6 * P.C, m = P.m, j = blockIdx.x * blockDim.x + threadIdx.x;
-  double v[2] = {0, 0};  // p . Sp over camera rows, H_cf . p (focal row)
-  if (j < n) {
+  const uint32_t n = 6 * P.C, m = P.m;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t j = blockIdx.x * 32 + lane;
+  double s = 0;
+  if (j < m)
+    for (uint32_t g = warp; g < P.prod_blocks; g += 8) s += P.acc_part[size_t(g) * m + j];
+  part[warp][lane] = s;
+  __syncthreads();
+  double v[2] = {0, 0};  // p . Sp over camera rows, H_cf . p (the focal row's camera share)
+  if (warp == 0) {
     double sum = 0;
-    for (uint32_t g = 0; g < P.prod_blocks; g++) sum += P.acc_part[size_t(g) * m + j];
-    const uint32_t c = j / 6, r = j % 6;
-    const double* U = P.camU + 21 * size_t(c);
-    const double* pc = P.p + 6 * size_t(c);
-    double up = 0;
 #pragma unroll
-    for (int k = 0; k < 6; k++) up += U[sym6(r, k)] * pc[k];
-    double sp = up + sum;
-    if (SHARED) {
-      sp += P.camHcf[j] * P.p[m - 1];
-      v[1] = P.camHcf[j] * P.p[j];
+    for (int w = 0; w < 8; w++) sum += part[w][lane];
+    if (j < n) {
+      const uint32_t c = j / 6, r = j % 6;
+      const double* U = P.camU + 21 * size_t(c);
+      const double* pc = P.p + 6 * size_t(c);
+      double up = 0;
+#pragma unroll
+      for (int k = 0; k < 6; k++) up += U[sym6(r, k)] * pc[k];
+      double sp = up + sum;
+      if (SHARED) {
+        sp += P.camHcf[j] * P.p[m - 1];
+        v[1] = P.camHcf[j] * P.p[j];
+      }
+      P.Sp[j] = sp;
+      v[0] = P.p[j] * sp;
+    } else if (SHARED && j == n) {
+      P.Sp[n] = sum;  // the observation share of the focal row; completed by the last block
     }
-    P.Sp[j] = sp;
-    v[0] = P.p[j] * sp;
   }
   block_sum(v, red);
   if (threadIdx.x == 0) {
     P.blk_part[2 * blockIdx.x] = v[0];
     P.blk_part[2 * blockIdx.x + 1] = v[1];
-    __threadfence();
-    last = atomicAdd(P.ticket, 1u) == gridDim.x - 1;
   }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
+  if (!last_block(P.ticket)) return;
   double t[2] = {0, 0};
   for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
     t[0] += __ldcg(P.blk_part + 2 * b);
     t[1] += __ldcg(P.blk_part + 2 * b + 1);
   }
-  double f[1] = {0};
-  if (SHARED)
-    for (uint32_t g = threadIdx.x; g < P.prod_blocks; g += blockDim.x) f[0] += P.acc_part[size_t(g) * m + n];
   block_sum(t, red);
-  if (SHARED) block_sum(f, red);
-  __shared__ double den_s;
-  if (threadIdx.x == 0) {
-    double den = t[0];
-    if (SHARED) {
-      const double pf = P.p[n];
-      const double spf = P.state[S_FOCAL_DIAG] * pf + t[1] + f[0];
-      P.Sp[n] = spf;
-      den += pf * spf;
-    }
-    den_s = den;
-    *P.ticket = 0;
+  if (threadIdx.x != 0) return;
+  double* st = P.state;
+  double den = t[0];
+  if (SHARED) {
+    const double pf = P.p[n];
+    const double spf = st[S_FOCAL_DIAG] * pf + t[1] + __ldcg(P.Sp + n);
+    P.Sp[n] = spf;
+    den += pf * spf;
+  }
+  *P.ticket = 0;
+  const double alpha = st[S_RHO] / den;
+  if (!(den > 0) || !(fabs(alpha) < 1e20)) {
+    st[S_CG_ACTIVE] = 0;
+    st[S_CG_FAILED] = 1;
+    return;
+  }
+  st[S_ALPHA] = alpha;
+}
+
+__global__ void __launch_bounds__(kUpdateThreads) k_pcg_update(Params P) {
+  __shared__ double rs[kUpdateRows];
+  __shared__ double red[2 * (kUpdateThreads / 32)];
+  double* st = P.state;
+  if (st[S_CG_ACTIVE] == 0) return;
+  const double alpha = st[S_ALPHA];
+  const uint32_t row = blockIdx.x * kUpdateRows + threadIdx.x;
+  const bool mine = threadIdx.x < uint32_t(kUpdateRows) && row < P.m;
+  double rr = 0;
+  if (mine) {
+    P.x[row] += alpha * P.p[row];
+    rr = P.r[row] - alpha * __ldcg(P.Sp + row);
+    P.r[row] = rr;
+    rs[threadIdx.x] = rr;
   }
   __syncthreads();
-  pcg_advance(P, den_s, red);
+  double v[2] = {0, 0};  // r . r, z . r
+  if (mine) {
+    double zz;
+    if (P.shared && row == P.m - 1) {
+      zz = st[S_FOCAL_INV] * rr;
+    } else {
+      const uint32_t jr = row % 6, base = threadIdx.x - jr;
+      const double* Mi = P.camMinv + 36 * size_t(row / 6) + 6 * jr;
+      zz = Mi[0] * rs[base] + Mi[1] * rs[base + 1] + Mi[2] * rs[base + 2] + Mi[3] * rs[base + 3] +
+           Mi[4] * rs[base + 4] + Mi[5] * rs[base + 5];
+    }
+    P.z[row] = zz;
+    v[0] = rr * rr;
+    v[1] = zz * rr;
+  }
+  block_sum(v, red);
+  if (threadIdx.x == 0) {
+    P.blk_part[2 * blockIdx.x] = v[0];
+    P.blk_part[2 * blockIdx.x + 1] = v[1];
+  }
+  if (!last_block(P.ticket + 1)) return;
+  double t[2] = {0, 0};
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    t[0] += __ldcg(P.blk_part + 2 * b);
+    t[1] += __ldcg(P.blk_part + 2 * b + 1);
+  }
+  block_sum(t, red);
+  if (threadIdx.x != 0) return;
+  P.ticket[1] = 0;
+  const double residual = t[0], rho = t[1];
+  st[S_CG_STEPS] += 1;
+  st[S_CG_SOLVE_STEPS] += 1;
+  st[S_R2] = residual;
+  if (residual <= P.tol * P.tol * st[S_R0]) {
+    st[S_CG_ACTIVE] = 0;
+    st[S_CG_CONVERGED] = 1;
+  } else if (!(rho > 0)) {
+    st[S_CG_ACTIVE] = 0;
+    st[S_CG_FAILED] = 1;
+  } else {
+    st[S_BETA] = rho / st[S_RHO];
+    st[S_RHO] = rho;
+  }
+}
+
+__global__ void k_pcg_direction(Params P) {
+  if (P.state[S_CG_ACTIVE] == 0) return;
+  const double beta = P.state[S_BETA];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P.m) P.p[i] = P.z[i] + beta * P.p[i];
 }
 
 // ---- K14/K15/K16: the candidate cameras, the focal scale and the gauge --------------------------
@@ -970,7 +1031,10 @@ __global__ void k_pack(Params P) {
 
 // ---- launches ----------------------------------------------------------------------------------
 
-uint32_t product_finish_blocks(const Params& p) { return (6 * p.C + kFinishThreads - 1) / kFinishThreads; }
+uint32_t product_finish_blocks(const Params& p) {
+  const uint32_t a = (p.m + 31) / 32, b = (p.m + kUpdateRows - 1) / kUpdateRows;
+  return a > b ? a : b;
+}
 size_t product_smem_bytes(const Params& p) { return size_t(p.m) * sizeof(double); }
 uint32_t product_max_unknowns() { return (227 * 1024) / sizeof(double) - 64; }
 
@@ -1002,8 +1066,10 @@ void launch_product(const Params& p, cudaStream_t s) {
   else k_product<false><<<p.prod_blocks, kProductThreads, product_smem_bytes(p), s>>>(p);
 }
 void launch_product_finish(const Params& p, cudaStream_t s) {
-  if (p.shared) k_product_finish<true><<<product_finish_blocks(p), kFinishThreads, 0, s>>>(p);
-  else k_product_finish<false><<<product_finish_blocks(p), kFinishThreads, 0, s>>>(p);
+  if (p.shared) k_product_reduce<true><<<(p.m + 31) / 32, kReduceThreads, 0, s>>>(p);
+  else k_product_reduce<false><<<(p.m + 31) / 32, kReduceThreads, 0, s>>>(p);
+  k_pcg_update<<<(p.m + kUpdateRows - 1) / kUpdateRows, kUpdateThreads, 0, s>>>(p);
+  k_pcg_direction<<<(p.m + 255) / 256, 256, 0, s>>>(p);
 }
 void launch_update_cameras(const Params& p, cudaStream_t s) { k_update_cameras<<<1, 256, 0, s>>>(p); }
 void launch_update_points(const Params& p, cudaStream_t s) {
