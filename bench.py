@@ -69,14 +69,13 @@ def workload(scene, config, iterations):
             "l2": "working set larger than the 126 MB L2; no flush"}
 
 
-def product_bytes(scene, shared, prod_blocks):
-    """Algorithmic DRAM bytes of one launch of the one-pass Schur product k_product: per
-    observation its W block (18 words, 21 with the focal) and its camera and point indices; per
-    point V_p^-1 (6 words) and its offset; the direction vector p (m words) and the per-block
-    partial sums (prod_blocks x m words, written)."""
-    wdim = 21 if shared else 18
+def product_bytes(scene, shared, prod_blocks, factor_bytes=8):
+    """Algorithmic DRAM bytes of one launch of the one-pass Schur product k_product_f: per
+    observation its 12 stored Jacobian factors (8 B each in FP64, 4 B in the mixed form) and its
+    camera and point index (8 B); per point V_p^-1 (6 words) and its offset (4 B); the direction
+    vector p (m words) and the per-block partial rows (prod_blocks x m words, written)."""
     m = 6 * scene.C + (1 if shared else 0)
-    return scene.M * (8 * wdim + 8) + scene.P * (6 * 8 + 4) + 8 * m + 8 * m * prod_blocks
+    return scene.M * (12 * factor_bytes + 8) + scene.P * (6 * 8 + 4) + 8 * m + 8 * m * prod_blocks
 
 
 def two_pass_bytes(scene, shared):
@@ -297,7 +296,7 @@ def main():
     prod_n = sum(r["product_launches"] for r in reports)
     n_sms = torch.cuda.get_device_properties(local).multi_processor_count
     prod_blocks = n_sms  # one 512-thread block per SM (the product kernel's occupancy)
-    bytes_launch = product_bytes(scene, shared, prod_blocks)
+    bytes_launch = product_bytes(scene, shared, prod_blocks, 4 if args.precision == "mixed" else 8)
     t_launch = prod_ms / max(prod_n, 1) / 1000
     achieved = bytes_launch / t_launch / 1e9 if prod_n else None
     traffic = dram_traffic(scene, shared)
@@ -312,7 +311,7 @@ def main():
         "final_cost": final_cost, "final_rmse_px": final_rmse,
         "e2e": {"value": lm_all / e2e_max, "unit": UNIT, "h2d_bytes_per_step": int(reports[-1]["h2d_bytes"]),
                 "d2h_bytes_per_step": int(reports[-1]["d2h_bytes"])},
-        "roofline": {"bound": "hbm", "kernel": "k_product (one-pass Schur product S p)",
+        "roofline": {"bound": "hbm", "kernel": "k_product_f (one-pass Schur product S p over stored Jacobian factors)",
                      "achieved": achieved, "peak": pk["hbm_gbs"], "peak_kind": pk_kind, "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"] if achieved else None,
                      "traffic": traffic, "algorithmic_bytes": bytes_launch,

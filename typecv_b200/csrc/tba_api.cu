@@ -194,10 +194,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const uint32_t C = ctl->cameras, P = ctl->points, M = ctl->observations;
   const bool shared = ctl->shared_focal != 0;
   const uint32_t m = 6 * C + (shared ? 1 : 0);
-  if (m > tba::product_max_unknowns())
-    throw Fail{TBA_ERROR_BUDGET, "GPU BA reduced camera system exceeds the shared-memory budget of the Schur product (" +
-                                     std::to_string(m) + " unknowns, at most " +
-                                     std::to_string(tba::product_max_unknowns()) + ")"};
   const uint32_t* ps = index + 2 * size_t(M);
   const uint32_t* cs = ps + P + 1;
   const uint32_t* active = cs + C + 1 + M;
@@ -222,13 +218,18 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.stall = ctl->stall_tolerance;
   p.ntasks = ntasks;
   p.nchunks = nchunks;
-  p.wdim = shared ? 21 : 18;
   p.task_blocks = std::max<uint32_t>(1, std::min<uint32_t>(4 * d->sms, (ntasks + 7) / 8));
-  const size_t smem = tba::product_smem_bytes(p);
-  const int per_sm = tba::product_blocks_per_sm(smem);
-  p.prod_blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(per_sm * d->sms), (ntasks + 15) / 16));
   const uint32_t fblocks = tba::product_finish_blocks(p);
-
+  // The one-pass product over stored factors when its camera sums fit shared memory; the two-pass
+  // recompute form otherwise.  The mixed form stores FP32 factors.
+  const bool mixed = ctl->precision == TBA_PRECISION_MIXED;
+  p.factored = m <= tba::product_max_unknowns();
+  p.Mpad = (M + 31) / 32 * 32;
+  const size_t factor_bytes = p.factored ? size_t(tba::kFactors) * p.Mpad * (mixed ? 4 : 8) : 0;
+  p.F = nullptr;
+  p.F32 = mixed && p.factored ? reinterpret_cast<float*>(1) : nullptr;  // set below; selects the occupancy query
+  const int per_sm = p.factored ? tba::product_blocks_per_sm(p) : 1;
+  p.prod_blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(per_sm * d->sms), (ntasks + 15) / 16));
   Layout L;
   const size_t o_poses = L.take<double>(12 * size_t(C)), o_points = L.take<double>(3 * size_t(P)),
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
@@ -236,13 +237,15 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_index = L.take<uint32_t>(3 * size_t(M) + P + 2 * size_t(C) + 2),
                o_tasks = L.take<uint32_t>(tasks.size()), o_ccam = L.take<uint32_t>(nchunks),
                o_cbeg = L.take<uint32_t>(nchunks + 1), o_cfirst = L.take<uint32_t>(C + 1),
-               o_W = L.take<double>(size_t(p.wdim) * M), o_vinv = L.take<double>(6 * size_t(P)),
-               o_bp = L.take<double>(3 * size_t(P)), o_U = L.take<double>(21 * size_t(C)),
+               o_rlim = L.take<double>(C), o_cmp = L.take<uint32_t>(M), o_cmx = L.take<double>(2 * size_t(M)),
+               o_pblk = L.take<double>(12 * size_t(P)), o_y = L.take<double>(4 * size_t(P)),
+               o_cprod = L.take<double>(8 * size_t(nchunks)), o_F = L.take<char>(factor_bytes),
+               o_pw = L.take<double>(6 * size_t(C)), o_xw = L.take<double>(6 * size_t(C)),
+               o_acc = L.take<double>(p.factored ? size_t(p.prod_blocks) * m : 0), o_U = L.take<double>(21 * size_t(C)),
                o_Minv = L.take<double>(36 * size_t(C)), o_rhs = L.take<double>(6 * size_t(C)),
                o_hcf = L.take<double>(6 * size_t(C)),
                o_chunk = L.take<double>(size_t(tba::kCameraPartials) * nchunks),
-               o_vec = L.take<double>(5 * size_t(m)), o_acc = L.take<double>(size_t(p.prod_blocks) * m),
-               o_blk = L.take<double>(2 * size_t(fblocks)),
+               o_vec = L.take<double>(5 * size_t(m)), o_blk = L.take<double>(4 * size_t(fblocks)),
                o_scal = L.take<double>(size_t(tba::kScalarPartials) * p.task_blocks),
                o_cost = L.take<double>(4 * size_t(p.task_blocks)), o_ticket = L.take<uint32_t>(8),
                o_state = L.take<double>(tba::S_WORDS), o_out = L.take<double>(12 * size_t(C) + 3 * size_t(P) + 27);
@@ -279,10 +282,17 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.chunk_cam = U32(o_ccam);
   p.chunk_beg = U32(o_cbeg);
   p.cam_chunk = U32(o_cfirst);
-  p.W = D(o_W);
-  p.Wf32 = nullptr;
-  p.vinv = D(o_vinv);
-  p.bp = D(o_bp);
+  p.rlim = D(o_rlim);
+  p.cm_point = U32(o_cmp);
+  p.cm_pixel = D(o_cmx);
+  p.pblk = D(o_pblk);
+  p.y = D(o_y);
+  p.chunk_prod = D(o_cprod);
+  p.F = p.factored && !mixed ? D(o_F) : nullptr;
+  p.F32 = p.factored && mixed ? reinterpret_cast<float*>(a + o_F) : nullptr;
+  p.pw = D(o_pw);
+  p.xw = D(o_xw);
+  p.acc_part = D(o_acc);
   p.camU = D(o_U);
   p.camMinv = D(o_Minv);
   p.camRhs = D(o_rhs);
@@ -294,7 +304,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.p = vec + 2 * size_t(m);
   p.Sp = vec + 3 * size_t(m);
   p.z = vec + 4 * size_t(m);
-  p.acc_part = D(o_acc);
   p.blk_part = D(o_blk);
   p.scal_part = D(o_scal);
   p.cost_part = D(o_cost);
@@ -331,7 +340,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   tba::launch_initialize(p, s);
   tba::launch_cost(p, s);
   tba::launch_finish_metrics(p, s);
-  launches += 3;
+  launches += 4;
   CUDA_TRY(cudaGetLastError());
   bool lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
@@ -355,7 +364,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
           tba::launch_product(p, s);
         }
         tba::launch_product_finish(p, s);
-        launches += 4;
+        launches += 5;
       }
       CUDA_TRY(cudaGetLastError());
       done += k;

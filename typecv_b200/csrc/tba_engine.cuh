@@ -4,21 +4,21 @@
 //   * scene: poses 12C, points 3P, cameras 6C, pixels 2M (observations point-major, as the
 //     reference packs them), and the trial poses/points of the LM candidate;
 //   * index: the reference's packed index array (obsCamera, obsPoint, pointStart, cameraStart,
-//     cameraObservations, cameraActive);
-//   * per observation, the Schur cross blocks W_i = w J_c^T J_p (18 words; 21 with the shared
-//     focal, whose 3 words are w J_f^T J_p), stored component-major ([k][M]) so that a warp
-//     reading 32 consecutive observations reads 256 contiguous bytes per component;
-//   * per point, the inverse of the damped point block V_p (6 words, symmetric) and its
-//     right-hand side b_p (3), component-major;
+//     cameraObservations, cameraActive), plus camera-major copies of each observation's point and
+//     pixel so that camera passes stream instead of gathering;
+//   * per point, a 12-word record: the inverse of the damped point block V_p (6, symmetric), its
+//     right-hand side b_p (3) and padding; and y_p = V_p^-1 W^T p of the current product (4);
 //   * per camera, the damped block U_c (21, lower triangle), the block-Jacobi preconditioner
-//     (S_cc)^-1 (36), the reduced right-hand side (6) and the camera/focal coupling H_cf (6);
+//     (S_cc)^-1 (36), the reduced right-hand side (6), the camera/focal coupling H_cf (6) and the
+//     radial limit of its lens model;
 //   * the PCG vectors x, r, p, Sp, z of length m = 6C (+1 with the shared focal);
 //   * the LM/PCG state words of the reference (bundle-shared.ts:362-386) plus the focal scalars.
+// Nothing per observation is stored beyond the inputs: the Jacobian factors are recomputed.
 //
 // Work decomposition: observation-parallel "warp tasks" — runs of whole points of at most 32
 // observations, one observation per lane, reduced per point with warp-shuffle segmented scans;
 // a point with more than 32 observations is a task of its own, swept in rounds of 32.  Camera
-// reductions run over the camera-major observation list in chunks.
+// reductions run over the camera-major observation list in chunks of a fixed schedule.
 #pragma once
 
 #include <cstdint>
@@ -50,8 +50,10 @@ enum StateWord : int {
 };
 
 constexpr int kTaskObs = 32;        // observations per warp task (one per lane)
+constexpr int kFactors = 12;        // stored Jacobian factors per observation
+constexpr int kProductThreads = 384;  // two blocks per SM
+
 constexpr int kPointThreads = 256;  // threads of the task kernels
-constexpr int kProductThreads = 512;
 constexpr int kCameraThreads = 128;
 constexpr int kCameraPartials = 60;  // U 21 | b_c 6 | H_cf 6 | (W V^-1 W^T) 21 | W V^-1 b_p 6
 constexpr int kScalarPartials = 4;   // H_ff obs | b_f obs | focal diag point terms | focal rhs point terms
@@ -81,14 +83,24 @@ struct Params {
   const uint32_t* chunk_beg;    // nchunks + 1 positions in camera_obs
   const uint32_t* cam_chunk;    // C + 1 first chunk of each camera
   uint32_t nchunks;
-  uint32_t task_blocks;  // grid of the task kernels (point pass, update, cost)
-  uint32_t prod_blocks;  // grid of the Schur product kernel
+  uint32_t task_blocks;  // grid of the task kernels (point pass, Schur points, update, cost)
   // linearisation
-  double* W;     // wdim * M, component-major
-  uint32_t wdim; // 18 or 21
-  float* Wf32;   // mixed precision copy, wdim * M (or null)
-  double* vinv;  // 6P
-  double* bp;    // 3P
+  double* rlim;        // C radial limits
+  uint32_t* cm_point;  // M, camera-major
+  double* cm_pixel;    // 2M, camera-major
+  double* pblk;        // 12P: V^-1 (6), b_p (3), padding
+  double* y;           // 4P: y_p of the current Schur product
+  double* chunk_prod;  // 8 per camera chunk: sum W_i y (6), focal share
+  // Jacobian factors of each observation (factored engine), component-major [12][Mpad]:
+  // q~ = R^T q (3), J_p rows R^T du, R^T dv (6), Huber weight, focal column jf (2).
+  double* F;
+  float* F32;          // the same factors in FP32 (mixed precision), or null
+  uint32_t Mpad;       // stride of a factor component
+  uint32_t factored;   // 1: one-pass product over stored factors; 0: two-pass recompute
+  uint32_t prod_blocks;  // grid of the one-pass product
+  double* pw;          // 6C: the PCG direction of each camera in world axes (R^T omega, R^T v)
+  double* xw;          // 6C: the PCG solution of each camera in world axes
+  double* acc_part;    // prod_blocks x m: per-block camera sums of the one-pass product
   double* camU;     // 21C
   double* camMinv;  // 36C
   double* camRhs;   // 6C
@@ -100,8 +112,7 @@ struct Params {
   double* p;
   double* Sp;
   double* z;
-  double* acc_part;   // product partials, gridDim * m
-  double* blk_part;   // finish partials, 2 per block
+  double* blk_part;   // finish partials, 4 per block
   double* scal_part;  // kScalarPartials per block of the task kernels
   double* cost_part;  // 4 per block
   uint32_t* ticket;   // last-block counters
@@ -126,15 +137,13 @@ void launch_update_points(const Params& p, cudaStream_t s);
 void launch_accept(const Params& p, cudaStream_t s);
 void launch_commit(const Params& p, cudaStream_t s);
 void launch_pack(const Params& p, cudaStream_t s);
-// Blocks of the widest finish kernel (sizes blk_part), and the dynamic shared memory of the
-// product kernel.
+// Blocks of the widest PCG-step kernel (sizes blk_part).
 uint32_t product_finish_blocks(const Params& p);
-size_t product_smem_bytes(const Params& p);
-// Largest unknown count whose accumulators fit one block's shared memory.
+// The one-pass product keeps m camera sums in shared memory: the largest m it takes, its
+// dynamic shared memory, the opt-in of the product kernels, and their blocks per SM.
 uint32_t product_max_unknowns();
-// Opt the product kernel into its shared-memory size; returns the first CUDA error.
+size_t product_smem_bytes(const Params& p);
 cudaError_t configure_kernels();
-// Blocks per SM of the product kernel at `smem` bytes (occupancy query).
-int product_blocks_per_sm(size_t smem);
+int product_blocks_per_sm(const Params& p);
 
 }  // namespace tba

@@ -1,45 +1,48 @@
 // Kernels of the grid engine (one bundle adjustment over the whole GPU), sm_100a, FP64.
 //
-// Kernel                 reference kernel(s) it replaces (src/sfm/bundle/gpu/*.shade.ts)
-// k_initialize           initializeBundle (K1)
+// Kernel                  reference kernel(s) it replaces (src/sfm/bundle/gpu/*.shade.ts)
+// k_initialize, k_setup   initializeBundle (K1); per-camera radial limits and the camera-major
+//                         copies of the observations' point and pixel
 // k_cost/k_finish_metrics bundleMetricPartials + finishBundleMetrics (K3/K4)
-// k_point_pass           linearizeBundle + bundlePointBlocks + bundleFocalObservations +
-//                        bundleFocalPoints (K2/K5/K21)
-// k_camera_pass/_finish  bundleCameraRows + bundleFocalCameraRows + invertBundleCameraColumns +
-//                        finalizeBundleCameraInverse (K6/K8/K21)
-// k_pcg_init             dampBundleFocal + initializeBundleCg (K9/K21)
-// k_product/_finish      bundleSchurPoint + bundleSchurCamera (+ focal row) + advanceBundleCg
-//                        (K10/K11/K12): one pass over W with per-block shared-memory camera
-//                        accumulators, then a reduction of the block partials whose last block
-//                        runs the PCG step
-// k_update_cameras       updateBundleCandidate (cameras, focal) + bundleCandidateGauge +
-//                        normalizeBundleCandidate (cameras) (K14/K15/K16)
-// k_update_points        updateBundleCandidate (points) + normalizeBundleCandidate (points) +
-//                        bundleCandidatePartials (K14/K16/K17)
-// k_accept/k_commit      acceptBundleCandidate + commitBundleCandidate (K18/K19)
-// k_pack                 packBundleResult (K20)
+// k_point_pass            linearizeBundle + bundlePointBlocks + bundleFocalObservations +
+//                         bundleFocalPoints (K2/K5/K21)
+// k_camera_pass/_finish   bundleCameraRows + bundleFocalCameraRows + invertBundleCameraColumns +
+//                         finalizeBundleCameraInverse (K6/K8/K21)
+// k_pcg_init              dampBundleFocal + initializeBundleCg (K9/K21)
+// k_product_f             bundleSchurPoint + bundleSchurCamera (K10/K11) in one pass over the
+//                         stored world-axis Jacobian factors, camera sums in shared memory
+// k_product_columns       the fixed-order sum of the product blocks' partial rows
+// k_schur_points          (two-pass form, for camera systems too large for shared memory)
+//                         bundleSchurPoint (K10): y_p = V_p^-1 sum_i W_i^T p, point-major
+// k_schur_cameras         bundleSchurCamera (K11): sum_i W_i y_p per camera chunk, camera-major
+// k_product_reduce,       advanceBundleCg (K12), split into a reduction with alpha, a
+// k_pcg_update/_direction distributed update with beta, and the new direction
+// k_update_cameras        updateBundleCandidate (cameras, focal) + bundleCandidateGauge +
+//                         normalizeBundleCandidate (cameras) (K14/K15/K16)
+// k_update_points         updateBundleCandidate (points) + normalizeBundleCandidate (points) +
+//                         bundleCandidatePartials (K14/K16/K17)
+// k_accept/k_commit       acceptBundleCandidate + commitBundleCandidate (K18/K19)
+// k_pack                  packBundleResult (K20)
 //
-// Every reduction runs in a fixed order (fixed grids, fixed trees), so a solve is reproducible
-// run to run, except the shared-memory accumulation of the Schur product, whose FP64 atomic
-// adds commute only up to rounding.
+// No kernel stores the Schur cross blocks W_i = w J_c^T J_p (21 words per observation).  The
+// point pass stores 12 world-axis Jacobian factors per observation instead (q~ = R^T q, R^T du,
+// R^T dv, w, jf; FP64, or FP32 in the mixed form), from which every product is a few dozen FMAs;
+// the camera passes recompute the factors from the pose, the camera, the point and the pixel.
+// Every reduction runs in a fixed order (fixed grids, fixed trees, fixed chunking), except the
+// shared-memory camera sums of k_product_f, whose FP64 atomic adds commute only up to rounding.
 #include <cuda_runtime.h>
 
 #include "tba_engine.cuh"
 
-// Compile-time tuning of the heavy kernels (occupancy floors of __launch_bounds__, and whether
-// the Schur product keeps a lane's W block in registers between its two uses or re-reads it
-// from L1 for the scatter).
-#ifndef TBA_PRODUCT_MIN_BLOCKS
-#define TBA_PRODUCT_MIN_BLOCKS 2
-#endif
-#ifndef TBA_PRODUCT_RELOAD
-#define TBA_PRODUCT_RELOAD 1
-#endif
+// Compile-time tuning: occupancy floors of __launch_bounds__ for the heavy kernels.
 #ifndef TBA_POINT_MIN_BLOCKS
 #define TBA_POINT_MIN_BLOCKS 2
 #endif
 #ifndef TBA_CAMERA_MIN_BLOCKS
 #define TBA_CAMERA_MIN_BLOCKS 3
+#endif
+#ifndef TBA_SCHUR_MIN_BLOCKS
+#define TBA_SCHUR_MIN_BLOCKS 2
 #endif
 
 namespace tba {
@@ -47,25 +50,28 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ inline Camera camera_at(const Params& P, uint32_t c, double log_scale) {
-  const double* k = P.cams + 6 * size_t(c);
-  Camera cam{k[0], k[1], k[2], k[3], k[4], k[5]};
-  if (P.shared) {
-    const double s = exp(log_scale);
-    cam.fx *= s;
-    cam.fy *= s;
-  }
-  return cam;
+// The camera record with the accepted (or candidate) focal scale applied.
+__device__ inline Camera camera_at(const Params& P, uint32_t c, double fscale) {
+  const double2* k = reinterpret_cast<const double2*>(P.cams + 6 * size_t(c));
+  const double2 a = k[0], b = k[1], e = k[2];
+  return Camera{a.x * fscale, a.y * fscale, b.x, b.y, e.x, e.y};
 }
 
-__device__ inline void load_pose(const double* poses, uint32_t c, double out[12]) {
-  const double2* src = reinterpret_cast<const double2*>(poses + 12 * size_t(c));
+__device__ inline double focal_scale(const Params& P, double log_scale) { return P.shared ? exp(log_scale) : 1.0; }
+
+__device__ inline void load6(const double* src, double out[6]) {
+  const double2* s = reinterpret_cast<const double2*>(src);
 #pragma unroll
-  for (int k = 0; k < 6; k++) {
-    const double2 v = src[k];
+  for (int k = 0; k < 3; k++) {
+    const double2 v = s[k];
     out[2 * k] = v.x;
     out[2 * k + 1] = v.y;
   }
+}
+
+__device__ inline void load_pose(const double* poses, uint32_t c, double out[12]) {
+  load6(poses + 12 * size_t(c), out);
+  load6(poses + 12 * size_t(c) + 6, out + 6);
 }
 
 // Inclusive segmented sum over lanes: lanes with equal `seg` form contiguous runs.
@@ -123,7 +129,36 @@ __device__ inline void block_tasks(const Params& P, uint32_t& begin, uint32_t& e
 
 __device__ inline bool directional(const Params& P, uint32_t pt) { return pt >= P.P - P.D; }
 
-// ---- K1: initializeBundle ----------------------------------------------------------------------
+// The point-major observation i of point pt: its Jacobian factors at the accepted scene.
+__device__ inline bool observe(const Params& P, uint32_t i, uint32_t c, uint32_t pt, double fscale, double pose[12],
+                               Geo& g) {
+  load_pose(P.poses, c, pose);
+  const Camera k = camera_at(P, c, fscale);
+  const double2 uv = reinterpret_cast<const double2*>(P.pixels)[i];
+  return geometry(pose, k, P.rlim[c], P.points + 3 * size_t(pt), directional(P, pt), uv.x, uv.y, P.huber, g);
+}
+
+// The camera's 6-vector v in world axes: (R^T v_omega, R^T v_t).
+__device__ inline void to_world(const double* R, const double v[6], double* out) {
+  for (int c = 0; c < 3; c++) {
+    out[c] = R[c] * v[0] + R[3 + c] * v[1] + R[6 + c] * v[2];
+    out[3 + c] = R[c] * v[3] + R[3 + c] * v[4] + R[6 + c] * v[5];
+  }
+}
+
+// True in the block that finishes last.  Every thread fences its own writes before the barrier,
+// so the last block sees every block's results (read them with __ldcg).
+__device__ inline bool last_block(uint32_t* ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// ---- K1: initializeBundle, and the per-solve set-up -----------------------------------------------
 
 __global__ void k_initialize(Params P) {
   double* st = P.state;
@@ -148,36 +183,32 @@ __global__ void k_initialize(Params P) {
   for (int k = 0; k < 8; k++) P.ticket[k] = 0;
 }
 
+// Per-camera radial limits; the camera-major copies of each observation's point and pixel.
+__global__ void k_setup(Params P) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < P.C) P.rlim[k] = radial_limit(P.cams[6 * size_t(k) + 4], P.cams[6 * size_t(k) + 5]);
+  if (k < P.M) {
+    const uint32_t i = P.camera_obs[k];
+    P.cm_point[k] = P.obs_point[i];
+    reinterpret_cast<double2*>(P.cm_pixel)[k] = reinterpret_cast<const double2*>(P.pixels)[i];
+  }
+}
+
 // ---- K3/K4: the linearised cost of the scene ---------------------------------------------------
 
 __global__ void __launch_bounds__(kPointThreads) k_cost(Params P) {
   __shared__ double red[3 * (kPointThreads / 32)];
   double v[3] = {0, 0, 0};  // cost, squared error, invalid projections
-  const double logf = P.state[S_LOG_FOCAL];
+  const double fscale = focal_scale(P, P.state[S_LOG_FOCAL]);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.M; i += gridDim.x * blockDim.x) {
-    const uint32_t c = P.obs_camera[i], pt = P.obs_point[i];
     double pose[12];
-    load_pose(P.poses, c, pose);
-    const Camera k = camera_at(P, c, logf);
-    const double* X = P.points + 3 * size_t(pt);
-    const double2 uv = reinterpret_cast<const double2*>(P.pixels)[i];
-    double cost, sq;
-    double q[3];
-    const bool dir = directional(P, pt);
-    for (int j = 0; j < 3; j++) {
-      q[j] = pose[j * 3] * X[0] + pose[j * 3 + 1] * X[1] + pose[j * 3 + 2] * X[2];
-      if (!dir) q[j] += pose[9 + j];
-    }
-    double pixel[2], du[3], dv[3];
-    if (!project(k, q, pixel, du, dv)) {
+    Geo g;
+    if (!observe(P, i, P.obs_camera[i], P.obs_point[i], fscale, pose, g)) {
       v[2] += 1;
       continue;
     }
-    const double ru = pixel[0] - uv.x, rv = pixel[1] - uv.y;
-    sq = ru * ru + rv * rv;
-    cost = robust_cost(sqrt(sq), P.huber);
-    v[0] += cost;
-    v[1] += sq;
+    v[0] += robust_cost(sqrt(g.sq), P.huber);
+    v[1] += g.sq;
   }
   block_sum(v, red);
   if (threadIdx.x == 0)
@@ -204,50 +235,53 @@ __global__ void k_finish_metrics(Params P) {
 
 // ---- K2/K5/K21: linearisation and point blocks -------------------------------------------------
 
-// One observation of the point pass: its contributions to the point block (V 6 unique,
-// b_p 3, focal cross sum 3, invalid 1) and its W_i, written to the component-major store.
+// One observation's contributions to its point block: V (6 unique), b_p (3), the focal cross sum
+// w J_p^T jf (3) and an invalid flag; and its share of the focal diagonal and right-hand side.
 template <bool SHARED>
-__device__ inline void point_obs(const Params& P, uint32_t i, uint32_t pt, double logf,
-                                 double (&v)[13], double& hff, double& bf) {
-  const uint32_t c = P.obs_camera[i];
+__device__ inline void point_obs(const Params& P, uint32_t i, uint32_t pt, double fscale, double (&v)[13],
+                                 double& hff, double& bf) {
   double pose[12];
-  load_pose(P.poses, c, pose);
-  const Camera k = camera_at(P, c, logf);
-  const double* X = P.points + 3 * size_t(pt);
-  const double2 uv = reinterpret_cast<const double2*>(P.pixels)[i];
-  ObsLin o;
-  const size_t M = P.M;
-  if (!linearize(pose, k, X, P.active[c] != 0, directional(P, pt), uv.x, uv.y, P.huber, o)) {
+  Geo g;
+  if (!observe(P, i, P.obs_camera[i], pt, fscale, pose, g)) {
     v[12] = 1;
-    for (uint32_t n = 0; n < P.wdim; n++) P.W[n * M + i] = 0;
     return;
   }
-  const double w = o.w;
-  double wjp[2][3];
-#pragma unroll
-  for (int row = 0; row < 2; row++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) wjp[row][j] = w * o.jp[row][j];
-  v[0] = wjp[0][0] * o.jp[0][0] + wjp[1][0] * o.jp[1][0];
-  v[1] = wjp[0][0] * o.jp[0][1] + wjp[1][0] * o.jp[1][1];
-  v[2] = wjp[0][0] * o.jp[0][2] + wjp[1][0] * o.jp[1][2];
-  v[3] = wjp[0][1] * o.jp[0][1] + wjp[1][1] * o.jp[1][1];
-  v[4] = wjp[0][1] * o.jp[0][2] + wjp[1][1] * o.jp[1][2];
-  v[5] = wjp[0][2] * o.jp[0][2] + wjp[1][2] * o.jp[1][2];
-#pragma unroll
-  for (int j = 0; j < 3; j++) v[6 + j] = -(wjp[0][j] * o.r[0] + wjp[1][j] * o.r[1]);
-#pragma unroll
-  for (int kk = 0; kk < 6; kk++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) P.W[(kk * 3 + j) * M + i] = o.jc[0][kk] * wjp[0][j] + o.jc[1][kk] * wjp[1][j];
-  if (SHARED) {
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      v[9 + j] = o.jf[0] * wjp[0][j] + o.jf[1] * wjp[1][j];
-      P.W[(18 + j) * M + i] = v[9 + j];
+  double jp[2][3];
+  for (int c = 0; c < 3; c++) {
+    jp[0][c] = g.du[0] * pose[c] + g.du[1] * pose[3 + c] + g.du[2] * pose[6 + c];
+    jp[1][c] = g.dv[0] * pose[c] + g.dv[1] * pose[3 + c] + g.dv[2] * pose[6 + c];
+  }
+  if (P.factored) {
+    // The world-axis factors of the products: q~ = R^T q, R^T du, R^T dv, w, jf.
+    double f[kFactors];
+    for (int c = 0; c < 3; c++) {
+      f[c] = g.q[0] * pose[c] + g.q[1] * pose[3 + c] + g.q[2] * pose[6 + c];
+      f[3 + c] = jp[0][c];
+      f[6 + c] = jp[1][c];
     }
-    hff += w * (o.jf[0] * o.jf[0] + o.jf[1] * o.jf[1]);
-    bf += w * (o.jf[0] * o.r[0] + o.jf[1] * o.r[1]);
+    f[9] = g.w;
+    f[10] = g.jf[0];
+    f[11] = g.jf[1];
+    const size_t stride = P.Mpad;
+    if (P.F32)
+      for (int k = 0; k < kFactors; k++) P.F32[k * stride + i] = float(f[k]);
+    else
+      for (int k = 0; k < kFactors; k++) P.F[k * stride + i] = f[k];
+  }
+  double wjp[2][3];
+  for (int row = 0; row < 2; row++)
+    for (int j = 0; j < 3; j++) wjp[row][j] = g.w * jp[row][j];
+  v[0] = wjp[0][0] * jp[0][0] + wjp[1][0] * jp[1][0];
+  v[1] = wjp[0][0] * jp[0][1] + wjp[1][0] * jp[1][1];
+  v[2] = wjp[0][0] * jp[0][2] + wjp[1][0] * jp[1][2];
+  v[3] = wjp[0][1] * jp[0][1] + wjp[1][1] * jp[1][1];
+  v[4] = wjp[0][1] * jp[0][2] + wjp[1][1] * jp[1][2];
+  v[5] = wjp[0][2] * jp[0][2] + wjp[1][2] * jp[1][2];
+  for (int j = 0; j < 3; j++) v[6 + j] = -(wjp[0][j] * g.r[0] + wjp[1][j] * g.r[1]);
+  if (SHARED) {
+    for (int j = 0; j < 3; j++) v[9 + j] = g.jf[0] * wjp[0][j] + g.jf[1] * wjp[1][j];
+    hff += g.w * (g.jf[0] * g.jf[0] + g.jf[1] * g.jf[1]);
+    bf += g.w * (g.jf[0] * g.r[0] + g.jf[1] * g.r[1]);
   }
 }
 
@@ -260,15 +294,17 @@ __device__ inline void point_finish(const Params& P, uint32_t pt, const double (
   for (int j = 0; j < 3; j++) V[j * 4] += lambda * fmax(V[j * 4], 1e-10);
   double inv[6];
   const bool ok = v[12] == 0 && inverse3_spd(V, inv);
-  const size_t Pn = P.P;
+  double2* blk = reinterpret_cast<double2*>(P.pblk + 12 * size_t(pt));
   if (!ok) {
     P.state[S_POINT_FAILED] = 1;
-    for (int k = 0; k < 6; k++) P.vinv[k * Pn + pt] = 0;
-    for (int k = 0; k < 3; k++) P.bp[k * Pn + pt] = 0;
+    for (int k = 0; k < 6; k++) blk[k] = make_double2(0, 0);
     return;
   }
-  for (int k = 0; k < 6; k++) P.vinv[k * Pn + pt] = inv[k];
-  for (int k = 0; k < 3; k++) P.bp[k * Pn + pt] = v[6 + k];
+  blk[0] = make_double2(inv[0], inv[1]);
+  blk[1] = make_double2(inv[2], inv[3]);
+  blk[2] = make_double2(inv[4], inv[5]);
+  blk[3] = make_double2(v[6], v[7]);
+  blk[4] = make_double2(v[8], 0);
   if (SHARED) {
     const double I[9] = {inv[0], inv[1], inv[2], inv[1], inv[3], inv[4], inv[2], inv[4], inv[5]};
     for (int j = 0; j < 3; j++) {
@@ -283,7 +319,7 @@ template <bool SHARED>
 __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_pass(Params P) {
   __shared__ double red[kScalarPartials * (kPointThreads / 32)];
   if (P.state[S_ACTIVE] == 0) return;
-  const double lambda = P.state[S_LAMBDA], logf = P.state[S_LOG_FOCAL];
+  const double lambda = P.state[S_LAMBDA], fscale = focal_scale(P, P.state[S_LOG_FOCAL]);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   double sc[kScalarPartials] = {0, 0, 0, 0};  // hff, bf, diag_pt, rhs_pt (lane-local)
   uint32_t tb, te;
@@ -298,7 +334,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
       if (uint32_t(lane) < n) {
         pt = P.obs_point[o0 + lane];
         seg = int(pt - p0);
-        point_obs<SHARED>(P, o0 + lane, pt, logf, v, sc[0], sc[1]);
+        point_obs<SHARED>(P, o0 + lane, pt, fscale, v, sc[0], sc[1]);
       }
       seg_scan(v, seg, lane);
       const int next = __shfl_down_sync(kFull, seg, 1);
@@ -309,7 +345,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
       for (uint32_t base = 0; base < n; base += kTaskObs) {
         if (base + lane < n) {
           double u[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-          point_obs<SHARED>(P, o0 + base + lane, p0, logf, u, sc[0], sc[1]);
+          point_obs<SHARED>(P, o0 + base + lane, p0, fscale, u, sc[0], sc[1]);
           for (int k = 0; k < 13; k++) v[k] += u[k];
         }
       }
@@ -324,6 +360,14 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
 
 // ---- K6/K8/K21: camera blocks ------------------------------------------------------------------
 
+// The camera rows of one observation: J_c (zero translation for a bearing).
+__device__ inline void camera_rows(const Geo& g, bool dir, double jc[2][6]) {
+  pose_row(g.q, g.du, jc[0]);
+  pose_row(g.q, g.dv, jc[1]);
+  if (dir)
+    for (int c = 3; c < 6; c++) jc[0][c] = jc[1][c] = 0;
+}
+
 __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_camera_pass(Params P) {
   __shared__ double red[kCameraPartials * (kCameraThreads / 32)];
   if (P.state[S_ACTIVE] == 0) return;
@@ -332,26 +376,26 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_camer
   const uint32_t k0 = P.chunk_beg[ch], k1 = P.chunk_beg[ch + 1];
   double pose[12];
   load_pose(P.poses, c, pose);
-  const Camera cam = camera_at(P, c, P.state[S_LOG_FOCAL]);
-  const size_t Pn = P.P;
+  const Camera cam = camera_at(P, c, focal_scale(P, P.state[S_LOG_FOCAL]));
+  const double limit = P.rlim[c];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   // Pass 1: U_c (lower triangle), b_c, H_cf.
   {
     double a[33];
     for (int j = 0; j < 33; j++) a[j] = 0;
     for (uint32_t kk = k0 + threadIdx.x; kk < k1; kk += blockDim.x) {
-      const uint32_t i = P.camera_obs[kk], pt = P.obs_point[i];
-      const double2 uv = reinterpret_cast<const double2*>(P.pixels)[i];
-      ObsLin o;
-      if (!linearize(pose, cam, P.points + 3 * size_t(pt), true, directional(P, pt), uv.x, uv.y, P.huber, o))
+      const uint32_t pt = P.cm_point[kk];
+      const double2 uv = reinterpret_cast<const double2*>(P.cm_pixel)[kk];
+      Geo g;
+      if (!geometry(pose, cam, limit, P.points + 3 * size_t(pt), directional(P, pt), uv.x, uv.y, P.huber, g))
         continue;
-      double wjc[2][6];
-      for (int row = 0; row < 2; row++)
-        for (int j = 0; j < 6; j++) wjc[row][j] = o.w * o.jc[row][j];
+      double jc[2][6];
+      camera_rows(g, directional(P, pt), jc);
       for (int j = 0; j < 6; j++) {
-        for (int l = 0; l <= j; l++) a[sym6(j, l)] += wjc[0][j] * o.jc[0][l] + wjc[1][j] * o.jc[1][l];
-        a[21 + j] -= wjc[0][j] * o.r[0] + wjc[1][j] * o.r[1];
-        a[27 + j] += wjc[0][j] * o.jf[0] + wjc[1][j] * o.jf[1];
+        const double w0 = g.w * jc[0][j], w1 = g.w * jc[1][j];
+        for (int l = 0; l <= j; l++) a[sym6(j, l)] += w0 * jc[0][l] + w1 * jc[1][l];
+        a[21 + j] -= w0 * g.r[0] + w1 * g.r[1];
+        a[27 + j] += w0 * g.jf[0] + w1 * g.jf[1];
       }
     }
     for (int j = 0; j < 33; j++) {
@@ -365,24 +409,32 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_camer
     double b[27];
     for (int j = 0; j < 27; j++) b[j] = 0;
     for (uint32_t kk = k0 + threadIdx.x; kk < k1; kk += blockDim.x) {
-      const uint32_t i = P.camera_obs[kk], pt = P.obs_point[i];
-      const double2 uv = reinterpret_cast<const double2*>(P.pixels)[i];
-      ObsLin o;
-      if (!linearize(pose, cam, P.points + 3 * size_t(pt), true, directional(P, pt), uv.x, uv.y, P.huber, o))
+      const uint32_t pt = P.cm_point[kk];
+      const double2 uv = reinterpret_cast<const double2*>(P.cm_pixel)[kk];
+      Geo g;
+      if (!geometry(pose, cam, limit, P.points + 3 * size_t(pt), directional(P, pt), uv.x, uv.y, P.huber, g))
         continue;
+      double jc[2][6];
+      camera_rows(g, directional(P, pt), jc);
+      double jp[2][3];
+      for (int l = 0; l < 3; l++) {
+        jp[0][l] = g.w * (g.du[0] * pose[l] + g.du[1] * pose[3 + l] + g.du[2] * pose[6 + l]);
+        jp[1][l] = g.w * (g.dv[0] * pose[l] + g.dv[1] * pose[3 + l] + g.dv[2] * pose[6 + l]);
+      }
       double Wc[6][3];
       for (int j = 0; j < 6; j++)
-        for (int l = 0; l < 3; l++)
-          Wc[j][l] = o.jc[0][j] * (o.w * o.jp[0][l]) + o.jc[1][j] * (o.w * o.jp[1][l]);
-      const double v0 = P.vinv[pt], v1 = P.vinv[Pn + pt], v2 = P.vinv[2 * Pn + pt], v3 = P.vinv[3 * Pn + pt],
-                   v4 = P.vinv[4 * Pn + pt], v5 = P.vinv[5 * Pn + pt];
-      const double b0 = P.bp[pt], b1 = P.bp[Pn + pt], b2 = P.bp[2 * Pn + pt];
+        for (int l = 0; l < 3; l++) Wc[j][l] = jc[0][j] * jp[0][l] + jc[1][j] * jp[1][l];
+      double vb[6], bb[3];
+      load6(P.pblk + 12 * size_t(pt), vb);
+      bb[0] = P.pblk[12 * size_t(pt) + 6];
+      bb[1] = P.pblk[12 * size_t(pt) + 7];
+      bb[2] = P.pblk[12 * size_t(pt) + 8];
       for (int j = 0; j < 6; j++) {
-        const double t0 = Wc[j][0] * v0 + Wc[j][1] * v1 + Wc[j][2] * v2;
-        const double t1 = Wc[j][0] * v1 + Wc[j][1] * v3 + Wc[j][2] * v4;
-        const double t2 = Wc[j][0] * v2 + Wc[j][1] * v4 + Wc[j][2] * v5;
+        const double t0 = Wc[j][0] * vb[0] + Wc[j][1] * vb[1] + Wc[j][2] * vb[2];
+        const double t1 = Wc[j][0] * vb[1] + Wc[j][1] * vb[3] + Wc[j][2] * vb[4];
+        const double t2 = Wc[j][0] * vb[2] + Wc[j][1] * vb[4] + Wc[j][2] * vb[5];
         for (int l = 0; l <= j; l++) b[sym6(j, l)] += t0 * Wc[l][0] + t1 * Wc[l][1] + t2 * Wc[l][2];
-        b[21 + j] += t0 * b0 + t1 * b1 + t2 * b2;
+        b[21 + j] += t0 * bb[0] + t1 * bb[1] + t2 * bb[2];
       }
     }
     for (int j = 0; j < 27; j++) {
@@ -494,6 +546,12 @@ __global__ void __launch_bounds__(1024) k_pcg_init(Params P) {
     v[0] += rr * zz;
     v[1] += rr * rr;
   }
+  __syncthreads();
+  for (uint32_t c = threadIdx.x; c < P.C; c += blockDim.x) {
+    double pc[6];
+    for (int k = 0; k < 6; k++) pc[k] = P.p[6 * c + k];
+    to_world(P.poses + 12 * size_t(c), pc, P.pw + 6 * size_t(c));
+  }
   block_sum(v, red);
   if (threadIdx.x == 0) {
     st[S_RHO] = v[0];
@@ -503,108 +561,233 @@ __global__ void __launch_bounds__(1024) k_pcg_init(Params P) {
   }
 }
 
-// ---- K10/K11: the Schur product S p, one pass over W -------------------------------------------
+// ---- K10/K11: the Schur product S p ------------------------------------------------------------
+//
+// Pass 1, point-major (warp tasks): y_p = V_p^-1 sum_i W_i^T p_c(i) (+ W_f p_f), written per point.
+// Pass 2, camera-major (the camera chunks): sum_i W_i y_p(i) and the focal shares, per chunk.
+// W_i is recomputed in both passes; neither pass has atomics.
 
 template <bool SHARED>
-__global__ void __launch_bounds__(kProductThreads, TBA_PRODUCT_MIN_BLOCKS) k_product(Params P) {
-  extern __shared__ double acc[];
+__device__ inline void schur_point_obs(const Params& P, uint32_t i, uint32_t pt, double fscale, double pf,
+                                       double t[3]) {
+  const uint32_t c = P.obs_camera[i];
+  double pose[12];
+  Geo g;
+  if (!observe(P, i, c, pt, fscale, pose, g)) {
+    t[0] = t[1] = t[2] = 0;
+    return;
+  }
+  double xc[6];
+  load6(P.p + 6 * size_t(c), xc);
+  wt_product(g, pose, xc, pf, P.active[c] != 0, directional(P, pt), SHARED, t);
+}
+
+__device__ inline void schur_point_finish(const Params& P, uint32_t pt, const double s[3]) {
+  double vb[6];
+  load6(P.pblk + 12 * size_t(pt), vb);
+  double2* y = reinterpret_cast<double2*>(P.y + 4 * size_t(pt));
+  y[0] = make_double2(vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2], vb[1] * s[0] + vb[3] * s[1] + vb[4] * s[2]);
+  y[1] = make_double2(vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2], 0);
+}
+
+template <bool SHARED>
+__global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_schur_points(Params P) {
   if (P.state[S_CG_ACTIVE] == 0) return;
-  const uint32_t m = P.m;
-  for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) acc[j] = 0;
-  __syncthreads();
+  const double fscale = focal_scale(P, P.state[S_LOG_FOCAL]);
+  const double pf = SHARED ? P.p[P.m - 1] : 0.0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const size_t M = P.M, Pn = P.P;
-  const double* __restrict__ pv = P.p;
-  const double pf = SHARED ? pv[m - 1] : 0.0;
-  constexpr int WD = SHARED ? 21 : 18;
-  double ef = 0;  // focal row share of this lane
   uint32_t tb, te;
   block_tasks(P, tb, te);
   for (uint32_t t = tb + warp; t < te; t += nwarps) {
     const uint32_t p0 = P.tasks[t], p1 = P.tasks[t + 1];
     const uint32_t o0 = P.point_start[p0], n = P.point_start[p1] - o0;
     if (n <= uint32_t(kTaskObs)) {
-      const bool valid = uint32_t(lane) < n;
-      const uint32_t i = o0 + lane;
-      double w[WD];
       double s[3] = {0, 0, 0};
       int seg = -1 - lane;
-      uint32_t pt = 0, c = 0;
-      if (valid) {
-        pt = P.obs_point[i];
-        c = P.obs_camera[i];
+      uint32_t pt = 0;
+      if (uint32_t(lane) < n) {
+        pt = P.obs_point[o0 + lane];
         seg = int(pt - p0);
-#pragma unroll
-        for (int k = 0; k < WD; k++) w[k] = __ldg(P.W + k * M + i);
-        const double* xc = pv + 6 * size_t(c);
-        double x6[6];
-#pragma unroll
-        for (int k = 0; k < 6; k++) x6[k] = __ldg(xc + k);
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-          double a = SHARED ? w[18 + j] * pf : 0.0;
-#pragma unroll
-          for (int k = 0; k < 6; k++) a += w[k * 3 + j] * x6[k];
-          s[j] = a;
-        }
+        schur_point_obs<SHARED>(P, o0 + lane, pt, fscale, pf, s);
       }
       seg_scan(s, seg, lane);
-      // The last lane of each point forms y_p = V_p^-1 s_p; every lane of the point takes it.
-      double y[3] = {0, 0, 0};
-      if (valid && (uint32_t(lane) == n - 1 || __ldg(P.point_start + pt + 1) == i + 1)) {
-        const double v0 = __ldg(P.vinv + pt), v1 = __ldg(P.vinv + Pn + pt), v2 = __ldg(P.vinv + 2 * Pn + pt),
-                     v3 = __ldg(P.vinv + 3 * Pn + pt), v4 = __ldg(P.vinv + 4 * Pn + pt), v5 = __ldg(P.vinv + 5 * Pn + pt);
-        y[0] = v0 * s[0] + v1 * s[1] + v2 * s[2];
-        y[1] = v1 * s[0] + v3 * s[1] + v4 * s[2];
-        y[2] = v2 * s[0] + v4 * s[1] + v5 * s[2];
-      }
-      const int tail = valid ? int(__ldg(P.point_start + pt + 1) - 1 - o0) : lane;
-#pragma unroll
-      for (int j = 0; j < 3; j++) y[j] = __shfl_sync(kFull, y[j], tail);
-      if (valid) {
-        double* ac = acc + 6 * size_t(c);
-        if (TBA_PRODUCT_RELOAD) {
-#pragma unroll
-          for (int k = 0; k < WD; k++) w[k] = __ldg(P.W + k * M + i);
-        }
-#pragma unroll
-        for (int k = 0; k < 6; k++) atomicAdd(ac + k, -(w[k * 3] * y[0] + w[k * 3 + 1] * y[1] + w[k * 3 + 2] * y[2]));
-        if (SHARED) ef += w[18] * y[0] + w[19] * y[1] + w[20] * y[2];
-      }
+      const int next = __shfl_down_sync(kFull, seg, 1);
+      if (uint32_t(lane) < n && (uint32_t(lane) == n - 1 || next != seg)) schur_point_finish(P, pt, s);
     } else {
-      // A point with more than 32 observations: two sweeps over its observations.
-      const uint32_t pt = p0;
       double s[3] = {0, 0, 0};
-      for (uint32_t base = 0; base < n; base += kTaskObs) {
+      for (uint32_t base = 0; base < n; base += kTaskObs)
         if (base + lane < n) {
-          const uint32_t i = o0 + base + lane, c = P.obs_camera[i];
-          const double* xc = pv + 6 * size_t(c);
-#pragma unroll
-          for (int j = 0; j < 3; j++) {
-            double a = SHARED ? __ldg(P.W + (18 + j) * M + i) * pf : 0.0;
-#pragma unroll
-            for (int k = 0; k < 6; k++) a += __ldg(P.W + (k * 3 + j) * M + i) * __ldg(xc + k);
-            s[j] += a;
-          }
+          double u[3];
+          schur_point_obs<SHARED>(P, o0 + base + lane, p0, fscale, pf, u);
+          s[0] += u[0];
+          s[1] += u[1];
+          s[2] += u[2];
         }
-      }
       warp_allsum(s);
-      const double v0 = __ldg(P.vinv + pt), v1 = __ldg(P.vinv + Pn + pt), v2 = __ldg(P.vinv + 2 * Pn + pt),
-                   v3 = __ldg(P.vinv + 3 * Pn + pt), v4 = __ldg(P.vinv + 4 * Pn + pt), v5 = __ldg(P.vinv + 5 * Pn + pt);
-      const double y0 = v0 * s[0] + v1 * s[1] + v2 * s[2];
-      const double y1 = v1 * s[0] + v3 * s[1] + v4 * s[2];
-      const double y2 = v2 * s[0] + v4 * s[1] + v5 * s[2];
-      for (uint32_t base = 0; base < n; base += kTaskObs) {
-        if (base + lane < n) {
-          const uint32_t i = o0 + base + lane, c = P.obs_camera[i];
-          double* ac = acc + 6 * size_t(c);
-#pragma unroll
-          for (int k = 0; k < 6; k++)
-            atomicAdd(ac + k, -(__ldg(P.W + (k * 3) * M + i) * y0 + __ldg(P.W + (k * 3 + 1) * M + i) * y1 +
-                                __ldg(P.W + (k * 3 + 2) * M + i) * y2));
-          if (SHARED)
-            ef += __ldg(P.W + 18 * M + i) * y0 + __ldg(P.W + 19 * M + i) * y1 + __ldg(P.W + 20 * M + i) * y2;
-        }
+      if (lane == 0) schur_point_finish(P, p0, s);
+    }
+  }
+}
+
+template <bool SHARED>
+__global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur_cameras(Params P) {
+  __shared__ double red[7 * (kCameraThreads / 32)];
+  if (P.state[S_CG_ACTIVE] == 0) return;
+  const uint32_t ch = blockIdx.x, c = P.chunk_cam[ch];
+  const bool variable = P.active[c] != 0;
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};  // sum_i W_i y (6), focal share (1)
+  if (variable || SHARED) {
+    const uint32_t k0 = P.chunk_beg[ch], k1 = P.chunk_beg[ch + 1];
+    double pose[12];
+    load_pose(P.poses, c, pose);
+    const Camera cam = camera_at(P, c, focal_scale(P, P.state[S_LOG_FOCAL]));
+    const double limit = P.rlim[c];
+    for (uint32_t kk = k0 + threadIdx.x; kk < k1; kk += blockDim.x) {
+      const uint32_t pt = P.cm_point[kk];
+      const double2 uv = reinterpret_cast<const double2*>(P.cm_pixel)[kk];
+      Geo g;
+      const bool dir = directional(P, pt);
+      if (!geometry(pose, cam, limit, P.points + 3 * size_t(pt), dir, uv.x, uv.y, P.huber, g)) continue;
+      const double2* yp = reinterpret_cast<const double2*>(P.y + 4 * size_t(pt));
+      const double2 y01 = yp[0], y2 = yp[1];
+      const double y[3] = {y01.x, y01.y, y2.x};
+      double d[6], e;
+      w_product(g, pose, y, variable, dir, d, e);
+      for (int j = 0; j < 6; j++) v[j] += d[j];
+      v[6] += e;
+    }
+  }
+  block_sum(v, red);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < 7; j++) P.chunk_prod[8 * size_t(ch) + j] = v[j];
+}
+
+// ---- K10/K11, factored: the Schur product S p in one pass over the stored factors -------------
+//
+// Each warp task forms y_p = V_p^-1 sum_i W_i^T p for its points from the observations' factors
+// (one observation per lane, a segmented warp scan per point), then scatters -W_i y_p into this
+// block's copy of the camera sums in shared memory (world axes; FP64).  At the end the block
+// rotates each camera's sums into the camera's axes (R [q~ x h~; h~] = J_c^T g) and writes them
+// as one partial row; k_product_columns adds the rows in a fixed order.  T is the factors'
+// storage type: double for the FP64 form, float for the mixed form (the per-observation
+// arithmetic then runs in FP32 and every sum in FP64).
+
+template <typename T>
+struct Factors {
+  T q[3], ju[3], jv[3], w, jf[2];
+};
+
+template <typename T>
+__device__ inline void load_factors(const T* F, size_t stride, uint32_t i, Factors<T>& f) {
+  const T* p = F + i;
+  f.q[0] = __ldg(p); f.q[1] = __ldg(p + stride); f.q[2] = __ldg(p + 2 * stride);
+  f.ju[0] = __ldg(p + 3 * stride); f.ju[1] = __ldg(p + 4 * stride); f.ju[2] = __ldg(p + 5 * stride);
+  f.jv[0] = __ldg(p + 6 * stride); f.jv[1] = __ldg(p + 7 * stride); f.jv[2] = __ldg(p + 8 * stride);
+  f.w = __ldg(p + 9 * stride);
+  f.jf[0] = __ldg(p + 10 * stride); f.jf[1] = __ldg(p + 11 * stride);
+}
+
+// W_i^T x in world axes, from the factors and the camera's step in world axes (xw).
+template <typename T>
+__device__ inline void factor_wt(const Factors<T>& f, const double* xw, double xf, bool variable, bool dir, bool shared,
+                                 double t[3]) {
+  T au = 0, av = 0;
+  if (variable) {
+    const T o0 = T(xw[0]), o1 = T(xw[1]), o2 = T(xw[2]);
+    T m0 = o1 * f.q[2] - o2 * f.q[1], m1 = o2 * f.q[0] - o0 * f.q[2], m2 = o0 * f.q[1] - o1 * f.q[0];
+    if (!dir) {
+      m0 += T(xw[3]);
+      m1 += T(xw[4]);
+      m2 += T(xw[5]);
+    }
+    au = f.ju[0] * m0 + f.ju[1] * m1 + f.ju[2] * m2;
+    av = f.jv[0] * m0 + f.jv[1] * m1 + f.jv[2] * m2;
+  }
+  if (shared) {
+    au += f.jf[0] * T(xf);
+    av += f.jf[1] * T(xf);
+  }
+  au *= f.w;
+  av *= f.w;
+  for (int c = 0; c < 3; c++) t[c] = double(au * f.ju[c] + av * f.jv[c]);
+}
+
+template <bool SHARED, typename T>
+__global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
+  extern __shared__ double acc[];
+  if (P.state[S_CG_ACTIVE] == 0) return;
+  const uint32_t m = P.m;
+  for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) acc[j] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const T* FT = sizeof(T) == 4 ? reinterpret_cast<const T*>(P.F32) : reinterpret_cast<const T*>(P.F);
+  const size_t stride = P.Mpad;
+  const double pf = SHARED ? P.p[m - 1] : 0.0;
+  double ef = 0;
+  uint32_t tb, te;
+  block_tasks(P, tb, te);
+  for (uint32_t t = tb + warp; t < te; t += nwarps) {
+    const uint32_t p0 = P.tasks[t], p1 = P.tasks[t + 1];
+    const uint32_t o0 = P.point_start[p0], n = P.point_start[p1] - o0;
+    const uint32_t rounds = n <= uint32_t(kTaskObs) ? 1 : (n + kTaskObs - 1) / kTaskObs;
+    // One point-aligned run of up to 32 observations per round; a long point takes several.
+    double s[3] = {0, 0, 0};
+    int seg = -1 - lane;
+    uint32_t pt = 0;
+    for (uint32_t r = 0; r < rounds; r++) {
+      const uint32_t k = r * kTaskObs + lane;
+      if (k < n) {
+        const uint32_t i = o0 + k;
+        const uint32_t c = P.obs_camera[i];
+        pt = P.obs_point[i];
+        seg = int(pt - p0);
+        Factors<T> f;
+        load_factors(FT, stride, i, f);
+        double xw[6], u[3];
+        load6(P.pw + 6 * size_t(c), xw);
+        factor_wt(f, xw, pf, P.active[c] != 0, directional(P, pt), SHARED, u);
+        s[0] += u[0];
+        s[1] += u[1];
+        s[2] += u[2];
+      }
+    }
+    if (rounds == 1) seg_scan(s, seg, lane);
+    else warp_allsum(s);
+    const bool valid = uint32_t(lane) < n;
+    const int next = __shfl_down_sync(kFull, seg, 1);
+    const bool tail = rounds == 1 ? (valid && (uint32_t(lane) == n - 1 || next != seg)) : lane == 0;
+    double y[3] = {0, 0, 0};
+    if (tail) {
+      double vb[6];
+      load6(P.pblk + 12 * size_t(rounds == 1 ? pt : p0), vb);
+      y[0] = vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2];
+      y[1] = vb[1] * s[0] + vb[3] * s[1] + vb[4] * s[2];
+      y[2] = vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2];
+    }
+    const unsigned tails = __ballot_sync(kFull, tail);
+    const int src = rounds == 1 ? (valid ? __ffs(tails & (kFull << lane)) - 1 : lane) : 0;
+    for (int j = 0; j < 3; j++) y[j] = __shfl_sync(kFull, y[j], src);
+    const T y0 = T(y[0]), y1 = T(y[1]), y2 = T(y[2]);
+    for (uint32_t r = 0; r < rounds; r++) {
+      const uint32_t k = r * kTaskObs + lane;
+      if (k >= n) continue;
+      const uint32_t i = o0 + k;
+      const uint32_t c = P.obs_camera[i];
+      Factors<T> f;
+      load_factors(FT, stride, i, f);
+      const T gu = f.w * (f.ju[0] * y0 + f.ju[1] * y1 + f.ju[2] * y2);
+      const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
+      if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
+      if (P.active[c] == 0) continue;
+      const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
+      double* ac = acc + 6 * size_t(c);
+      atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
+      atomicAdd(ac + 1, -double(f.q[2] * h0 - f.q[0] * h2));
+      atomicAdd(ac + 2, -double(f.q[0] * h1 - f.q[1] * h0));
+      if (!directional(P, P.obs_point[i])) {
+        atomicAdd(ac + 3, -double(h0));
+        atomicAdd(ac + 4, -double(h1));
+        atomicAdd(ac + 5, -double(h2));
       }
     }
   }
@@ -613,41 +796,26 @@ __global__ void __launch_bounds__(kProductThreads, TBA_PRODUCT_MIN_BLOCKS) k_pro
     if (lane == 0) atomicAdd(acc + (m - 1), -ef);
   }
   __syncthreads();
+  // Rotate each camera's sums into its axes and write this block's partial row.
   double* out = P.acc_part + size_t(blockIdx.x) * m;
-  for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) out[j] = acc[j];
+  for (uint32_t c = threadIdx.x; c < P.C; c += blockDim.x) {
+    const double* a = acc + 6 * size_t(c);
+    const double* R = P.poses + 12 * size_t(c);
+    for (int r = 0; r < 3; r++) {
+      out[6 * c + r] = R[3 * r] * a[0] + R[3 * r + 1] * a[1] + R[3 * r + 2] * a[2];
+      out[6 * c + 3 + r] = R[3 * r] * a[3] + R[3 * r + 1] * a[4] + R[3 * r + 2] * a[5];
+    }
+  }
+  if (SHARED && threadIdx.x == 0) out[m - 1] = acc[m - 1];
 }
 
-// ---- K12: one PCG step, in three short kernels --------------------------------------------------
-//
-// k_product_reduce   column-parallel sum of the product blocks' partial rows (fixed order), the
-//                    camera rows of S p = U_c p_c + H_cf p_f - sum, their p . Sp share; its last
-//                    block adds the focal row and forms alpha = rho / p.Sp (with the reference's
-//                    breakdown checks).
-// k_pcg_update       x += alpha p, r -= alpha Sp, z = M^-1 r by camera blocks (252 rows per block,
-//                    so no camera straddles two blocks); its last block forms the residual, rho,
-//                    the convergence test and beta.
-// k_pcg_direction    p = z + beta p.
-
-constexpr int kReduceThreads = 256;  // 8 warps; 32 columns per block
-constexpr int kUpdateRows = 252;     // 42 cameras per block
-constexpr int kUpdateThreads = 256;
-
-// True in the block that finishes last.  Every thread fences its own writes before the barrier,
-// so the last block sees every block's results (read them with __ldcg).
-__device__ inline bool last_block(uint32_t* ticket) {
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (last) __threadfence();
-  return last;
-}
-
+// The column sums of the one-pass product's partial rows (fixed order), then the camera rows of
+// S p = U_c p_c + H_cf p_f + sum, their p . Sp share; the last block adds the focal row and forms
+// alpha (the reference's breakdown checks).
 template <bool SHARED>
-__global__ void __launch_bounds__(kReduceThreads) k_product_reduce(Params P) {
+__global__ void __launch_bounds__(256) k_product_columns(Params P) {
   __shared__ double part[8][33];
-  __shared__ double red[2 * (kReduceThreads / 32)];
+  __shared__ double red[2 * 8];
   if (P.state[S_CG_ACTIVE] == 0) return;
   const uint32_t n = 6 * P.C, m = P.m;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -657,7 +825,7 @@ __global__ void __launch_bounds__(kReduceThreads) k_product_reduce(Params P) {
     for (uint32_t g = warp; g < P.prod_blocks; g += 8) s += P.acc_part[size_t(g) * m + j];
   part[warp][lane] = s;
   __syncthreads();
-  double v[2] = {0, 0};  // p . Sp over camera rows, H_cf . p (the focal row's camera share)
+  double v[2] = {0, 0};
   if (warp == 0) {
     double sum = 0;
 #pragma unroll
@@ -677,19 +845,19 @@ __global__ void __launch_bounds__(kReduceThreads) k_product_reduce(Params P) {
       P.Sp[j] = sp;
       v[0] = P.p[j] * sp;
     } else if (SHARED && j == n) {
-      P.Sp[n] = sum;  // the observation share of the focal row; completed by the last block
+      P.Sp[n] = sum;
     }
   }
   block_sum(v, red);
   if (threadIdx.x == 0) {
-    P.blk_part[2 * blockIdx.x] = v[0];
-    P.blk_part[2 * blockIdx.x + 1] = v[1];
+    P.blk_part[4 * blockIdx.x] = v[0];
+    P.blk_part[4 * blockIdx.x + 1] = v[1];
   }
   if (!last_block(P.ticket)) return;
   double t[2] = {0, 0};
   for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-    t[0] += __ldcg(P.blk_part + 2 * b);
-    t[1] += __ldcg(P.blk_part + 2 * b + 1);
+    t[0] += __ldcg(P.blk_part + 4 * b);
+    t[1] += __ldcg(P.blk_part + 4 * b + 1);
   }
   block_sum(t, red);
   if (threadIdx.x != 0) return;
@@ -698,6 +866,77 @@ __global__ void __launch_bounds__(kReduceThreads) k_product_reduce(Params P) {
   if (SHARED) {
     const double pf = P.p[n];
     const double spf = st[S_FOCAL_DIAG] * pf + t[1] + __ldcg(P.Sp + n);
+    P.Sp[n] = spf;
+    den += pf * spf;
+  }
+  *P.ticket = 0;
+  const double alpha = st[S_RHO] / den;
+  if (!(den > 0) || !(fabs(alpha) < 1e20)) {
+    st[S_CG_ACTIVE] = 0;
+    st[S_CG_FAILED] = 1;
+    return;
+  }
+  st[S_ALPHA] = alpha;
+}
+
+// ---- K12: one PCG step, in three short kernels --------------------------------------------------
+//
+// k_product_reduce   per camera row: S p = U_c p_c + H_cf p_f - sum over the camera's chunks; the
+//                    p . Sp share; the focal row's shares; its last block completes the focal row
+//                    and forms alpha = rho / p.Sp (with the reference's breakdown checks).
+// k_pcg_update       x += alpha p, r -= alpha Sp, z = M^-1 r by camera blocks (252 rows per block,
+//                    so no camera straddles two blocks); its last block forms the residual, rho,
+//                    the convergence test and beta.
+// k_pcg_direction    p = z + beta p.
+
+constexpr int kReduceThreads = 256;
+constexpr int kUpdateRows = 252;  // 42 cameras per block
+constexpr int kUpdateThreads = 256;
+
+template <bool SHARED>
+__global__ void __launch_bounds__(kReduceThreads) k_product_reduce(Params P) {
+  __shared__ double red[3 * (kReduceThreads / 32)];
+  if (P.state[S_CG_ACTIVE] == 0) return;
+  const uint32_t n = 6 * P.C, m = P.m;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[3] = {0, 0, 0};  // p . Sp over camera rows, H_cf . p, observation share of the focal row
+  if (j < n) {
+    const uint32_t c = j / 6, r = j % 6;
+    double sum = 0;
+    for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum += P.chunk_prod[8 * size_t(ch) + r];
+    const double* U = P.camU + 21 * size_t(c);
+    double pc[6];
+    load6(P.p + 6 * size_t(c), pc);
+    double up = 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) up += U[sym6(r, k)] * pc[k];
+    double sp = up - sum;
+    if (SHARED) {
+      sp += P.camHcf[j] * P.p[m - 1];
+      v[1] = P.camHcf[j] * pc[r];
+    }
+    P.Sp[j] = sp;
+    v[0] = pc[r] * sp;
+  }
+  if (SHARED)
+    for (uint32_t ch = j; ch < P.nchunks; ch += gridDim.x * blockDim.x) v[2] += P.chunk_prod[8 * size_t(ch) + 6];
+  block_sum(v, red);
+  if (threadIdx.x == 0) {
+    P.blk_part[4 * blockIdx.x] = v[0];
+    P.blk_part[4 * blockIdx.x + 1] = v[1];
+    P.blk_part[4 * blockIdx.x + 2] = v[2];
+  }
+  if (!last_block(P.ticket)) return;
+  double t[3] = {0, 0, 0};
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (int k = 0; k < 3; k++) t[k] += __ldcg(P.blk_part + 4 * b + k);
+  block_sum(t, red);
+  if (threadIdx.x != 0) return;
+  double* st = P.state;
+  double den = t[0];
+  if (SHARED) {
+    const double pf = P.p[n];
+    const double spf = st[S_FOCAL_DIAG] * pf + t[1] - t[2];
     P.Sp[n] = spf;
     den += pf * spf;
   }
@@ -775,8 +1014,17 @@ __global__ void __launch_bounds__(kUpdateThreads) k_pcg_update(Params P) {
 __global__ void k_pcg_direction(Params P) {
   if (P.state[S_CG_ACTIVE] == 0) return;
   const double beta = P.state[S_BETA];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < P.m) P.p[i] = P.z[i] + beta * P.p[i];
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < P.C) {
+    double v[6];
+    for (int k = 0; k < 6; k++) {
+      v[k] = P.z[6 * c + k] + beta * P.p[6 * c + k];
+      P.p[6 * c + k] = v[k];
+    }
+    to_world(P.poses + 12 * size_t(c), v, P.pw + 6 * size_t(c));
+  } else if (c == P.C && P.shared) {
+    P.p[P.m - 1] = P.z[P.m - 1] + beta * P.p[P.m - 1];
+  }
 }
 
 // ---- K14/K15/K16: the candidate cameras, the focal scale and the gauge --------------------------
@@ -800,6 +1048,7 @@ __global__ void __launch_bounds__(256) k_update_cameras(Params P) {
   for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
     double pose[12], moved[12];
     for (int j = 0; j < 12; j++) pose[j] = P.poses[12 * size_t(c) + j];
+    to_world(pose, P.x + 6 * size_t(c), P.xw + 6 * size_t(c));
     if (P.active[c]) move_pose(pose, P.x + 6 * size_t(c), moved);
     else
       for (int j = 0; j < 12; j++) moved[j] = pose[j];
@@ -857,18 +1106,41 @@ __global__ void __launch_bounds__(256) k_update_cameras(Params P) {
   }
 }
 
+// W_i^T x of one observation for the candidate update: from the stored FP64 factors when the
+// engine keeps them, else recomputed in FP64 (the mixed form keeps only FP32 factors, and the
+// back-substitution stays FP64).
+__device__ inline void update_wt(const Params& P, uint32_t i, uint32_t c, uint32_t pt, double fscale, double xf,
+                                 bool shared, double t[3]) {
+  t[0] = t[1] = t[2] = 0;
+  if (P.factored && P.F) {
+    Factors<double> f;
+    load_factors(static_cast<const double*>(P.F), P.Mpad, i, f);
+    double xw[6];
+    load6(P.xw + 6 * size_t(c), xw);
+    factor_wt(f, xw, xf, P.active[c] != 0, directional(P, pt), shared, t);
+    return;
+  }
+  double pose[12], xc[6];
+  Geo g;
+  if (observe(P, i, c, pt, fscale, pose, g)) {
+    load6(P.x + 6 * size_t(c), xc);
+    wt_product(g, pose, xc, xf, P.active[c] != 0, directional(P, pt), shared, t);
+  }
+}
+
 // ---- K14/K16/K17: candidate points and the candidate cost ---------------------------------------
 
-template <bool SHARED>
+// The candidate point: X + V^-1 (b_p - sum_i W_i^T x), then the bearing or similarity
+// normalisation of the gauge.
 __device__ inline void candidate_point(const Params& P, uint32_t pt, const double s[3], double X[3]) {
-  const size_t Pn = P.P;
-  const double v0 = P.vinv[pt], v1 = P.vinv[Pn + pt], v2 = P.vinv[2 * Pn + pt], v3 = P.vinv[3 * Pn + pt],
-               v4 = P.vinv[4 * Pn + pt], v5 = P.vinv[5 * Pn + pt];
-  const double r0 = P.bp[pt] - s[0], r1 = P.bp[Pn + pt] - s[1], r2 = P.bp[2 * Pn + pt] - s[2];
+  double vb[6];
+  load6(P.pblk + 12 * size_t(pt), vb);
+  const double* bb = P.pblk + 12 * size_t(pt) + 6;
+  const double r0 = bb[0] - s[0], r1 = bb[1] - s[1], r2 = bb[2] - s[2];
   const double* X0 = P.points + 3 * size_t(pt);
-  X[0] = X0[0] + (v0 * r0 + v1 * r1 + v2 * r2);
-  X[1] = X0[1] + (v1 * r0 + v3 * r1 + v4 * r2);
-  X[2] = X0[2] + (v2 * r0 + v4 * r1 + v5 * r2);
+  X[0] = X0[0] + (vb[0] * r0 + vb[1] * r1 + vb[2] * r2);
+  X[1] = X0[1] + (vb[1] * r0 + vb[3] * r1 + vb[4] * r2);
+  X[2] = X0[2] + (vb[2] * r0 + vb[4] * r1 + vb[5] * r2);
   const double* st = P.state;
   if (directional(P, pt)) {
     const double norm = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
@@ -884,13 +1156,12 @@ __device__ inline void candidate_point(const Params& P, uint32_t pt, const doubl
   out[2] = X[2];
 }
 
-template <bool SHARED>
-__device__ inline void candidate_obs(const Params& P, uint32_t i, uint32_t pt, const double X[3], double logf,
+__device__ inline void candidate_obs(const Params& P, uint32_t i, uint32_t pt, const double X[3], double fscale_trial,
                                      double& cost, double& sq) {
   const uint32_t c = P.obs_camera[i];
   double pose[12];
   load_pose(P.tposes, c, pose);
-  const Camera k = camera_at(P, c, logf);
+  const Camera k = camera_at(P, c, fscale_trial);
   const double2 uv = reinterpret_cast<const double2*>(P.pixels)[i];
   double oc, os;
   candidate_cost(pose, k, X, directional(P, pt), uv.x, uv.y, P.huber, oc, os);
@@ -899,15 +1170,13 @@ __device__ inline void candidate_obs(const Params& P, uint32_t i, uint32_t pt, c
 }
 
 template <bool SHARED>
-__global__ void __launch_bounds__(kPointThreads) k_update_points(Params P) {
+__global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_update_points(Params P) {
   __shared__ double red[2 * (kPointThreads / 32)];
   const double* st = P.state;
   if (st[S_ACTIVE] == 0 || st[S_CG_FAILED] != 0 || st[S_TRIAL_VALID] == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const size_t M = P.M;
-  const double* __restrict__ xv = P.x;
-  const double xf = SHARED ? xv[P.m - 1] : 0.0;
-  const double logf = SHARED ? st[S_LOG_FOCAL_TRIAL] : 0.0;
+  const double fscale = focal_scale(P, st[S_LOG_FOCAL]), fscale_trial = focal_scale(P, st[S_LOG_FOCAL_TRIAL]);
+  const double xf = SHARED ? P.x[P.m - 1] : 0.0;
   double cs[2] = {0, 0};
   uint32_t tb, te;
   block_tasks(P, tb, te);
@@ -923,40 +1192,35 @@ __global__ void __launch_bounds__(kPointThreads) k_update_points(Params P) {
       if (valid) {
         pt = P.obs_point[i];
         seg = int(pt - p0);
-        const uint32_t c = P.obs_camera[i];
-        const double* xc = xv + 6 * size_t(c);
-        for (int j = 0; j < 3; j++) {
-          double a = SHARED ? P.W[(18 + j) * M + i] * xf : 0.0;
-          for (int k = 0; k < 6; k++) a += P.W[(k * 3 + j) * M + i] * xc[k];
-          s[j] = a;
-        }
+        update_wt(P, i, P.obs_camera[i], pt, fscale, xf, SHARED, s);
       }
       seg_scan(s, seg, lane);
+      const int next = __shfl_down_sync(kFull, seg, 1);
+      const bool tail = valid && (uint32_t(lane) == n - 1 || next != seg);
       double X[3] = {0, 0, 0};
-      const uint32_t end = valid ? P.point_start[pt + 1] : 0;
-      if (valid && end == i + 1) candidate_point<SHARED>(P, pt, s, X);
-      const int tail = valid ? int(end - 1 - o0) : lane;
-      for (int j = 0; j < 3; j++) X[j] = __shfl_sync(kFull, X[j], tail);
-      if (valid) candidate_obs<SHARED>(P, i, pt, X, logf, cs[0], cs[1]);
+      if (tail) candidate_point(P, pt, s, X);
+      const unsigned tails = __ballot_sync(kFull, tail);
+      const int src = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
+      for (int j = 0; j < 3; j++) X[j] = __shfl_sync(kFull, X[j], src);
+      if (valid) candidate_obs(P, i, pt, X, fscale_trial, cs[0], cs[1]);
     } else {
       const uint32_t pt = p0;
       double s[3] = {0, 0, 0};
       for (uint32_t base = 0; base < n; base += kTaskObs)
         if (base + lane < n) {
-          const uint32_t i = o0 + base + lane, c = P.obs_camera[i];
-          const double* xc = xv + 6 * size_t(c);
-          for (int j = 0; j < 3; j++) {
-            double a = SHARED ? P.W[(18 + j) * M + i] * xf : 0.0;
-            for (int k = 0; k < 6; k++) a += P.W[(k * 3 + j) * M + i] * xc[k];
-            s[j] += a;
-          }
+          const uint32_t i = o0 + base + lane;
+          double u[3];
+          update_wt(P, i, P.obs_camera[i], pt, fscale, xf, SHARED, u);
+          s[0] += u[0];
+          s[1] += u[1];
+          s[2] += u[2];
         }
       warp_allsum(s);
       double X[3] = {0, 0, 0};
-      if (lane == 0) candidate_point<SHARED>(P, pt, s, X);
+      if (lane == 0) candidate_point(P, pt, s, X);
       for (int j = 0; j < 3; j++) X[j] = __shfl_sync(kFull, X[j], 0);
       for (uint32_t base = 0; base < n; base += kTaskObs)
-        if (base + lane < n) candidate_obs<SHARED>(P, o0 + base + lane, pt, X, logf, cs[0], cs[1]);
+        if (base + lane < n) candidate_obs(P, o0 + base + lane, pt, X, fscale_trial, cs[0], cs[1]);
     }
   }
   block_sum(cs, red);
@@ -1032,26 +1296,41 @@ __global__ void k_pack(Params P) {
 // ---- launches ----------------------------------------------------------------------------------
 
 uint32_t product_finish_blocks(const Params& p) {
-  const uint32_t a = (p.m + 31) / 32, b = (p.m + kUpdateRows - 1) / kUpdateRows;
-  return a > b ? a : b;
+  const uint32_t a = (6 * p.C + kReduceThreads - 1) / kReduceThreads, b = (p.m + kUpdateRows - 1) / kUpdateRows;
+  const uint32_t c = (p.m + 31) / 32;
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
-size_t product_smem_bytes(const Params& p) { return size_t(p.m) * sizeof(double); }
+
 uint32_t product_max_unknowns() { return (227 * 1024) / sizeof(double) - 64; }
+size_t product_smem_bytes(const Params& p) { return size_t(p.m) * sizeof(double); }
 
 cudaError_t configure_kernels() {
   const int bytes = 227 * 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_product<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_product<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  };
+  set(reinterpret_cast<const void*>(k_product_f<false, double>));
+  set(reinterpret_cast<const void*>(k_product_f<true, double>));
+  set(reinterpret_cast<const void*>(k_product_f<false, float>));
+  set(reinterpret_cast<const void*>(k_product_f<true, float>));
   return e;
 }
 
-int product_blocks_per_sm(size_t smem) {
+int product_blocks_per_sm(const Params& p) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_product<true>, kProductThreads, smem) != cudaSuccess) return 1;
+  const void* f = p.F32 ? reinterpret_cast<const void*>(k_product_f<true, float>)
+                        : reinterpret_cast<const void*>(k_product_f<true, double>);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kProductThreads, product_smem_bytes(p)) != cudaSuccess)
+    return 1;
   return n > 0 ? n : 1;
 }
 
-void launch_initialize(const Params& p, cudaStream_t s) { k_initialize<<<1, 1, 0, s>>>(p); }
+void launch_initialize(const Params& p, cudaStream_t s) {
+  k_initialize<<<1, 1, 0, s>>>(p);
+  const uint32_t n = p.M > p.C ? p.M : p.C;
+  k_setup<<<(n + 255) / 256, 256, 0, s>>>(p);
+}
 void launch_cost(const Params& p, cudaStream_t s) { k_cost<<<p.task_blocks, kPointThreads, 0, s>>>(p); }
 void launch_finish_metrics(const Params& p, cudaStream_t s) { k_finish_metrics<<<1, 1024, 0, s>>>(p); }
 void launch_point_pass(const Params& p, cudaStream_t s) {
@@ -1062,14 +1341,36 @@ void launch_camera_pass(const Params& p, cudaStream_t s) { k_camera_pass<<<p.nch
 void launch_camera_finish(const Params& p, cudaStream_t s) { k_camera_finish<<<(p.C + 127) / 128, 128, 0, s>>>(p); }
 void launch_pcg_init(const Params& p, cudaStream_t s) { k_pcg_init<<<1, 1024, 0, s>>>(p); }
 void launch_product(const Params& p, cudaStream_t s) {
-  if (p.shared) k_product<true><<<p.prod_blocks, kProductThreads, product_smem_bytes(p), s>>>(p);
-  else k_product<false><<<p.prod_blocks, kProductThreads, product_smem_bytes(p), s>>>(p);
+  if (p.factored) {
+    const size_t smem = product_smem_bytes(p);
+    if (p.F32) {
+      if (p.shared) k_product_f<true, float><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
+      else k_product_f<false, float><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
+    } else {
+      if (p.shared) k_product_f<true, double><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
+      else k_product_f<false, double><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
+    }
+    return;
+  }
+  if (p.shared) {
+    k_schur_points<true><<<p.task_blocks, kPointThreads, 0, s>>>(p);
+    k_schur_cameras<true><<<p.nchunks, kCameraThreads, 0, s>>>(p);
+  } else {
+    k_schur_points<false><<<p.task_blocks, kPointThreads, 0, s>>>(p);
+    k_schur_cameras<false><<<p.nchunks, kCameraThreads, 0, s>>>(p);
+  }
 }
 void launch_product_finish(const Params& p, cudaStream_t s) {
-  if (p.shared) k_product_reduce<true><<<(p.m + 31) / 32, kReduceThreads, 0, s>>>(p);
-  else k_product_reduce<false><<<(p.m + 31) / 32, kReduceThreads, 0, s>>>(p);
+  if (p.factored) {
+    if (p.shared) k_product_columns<true><<<(p.m + 31) / 32, 256, 0, s>>>(p);
+    else k_product_columns<false><<<(p.m + 31) / 32, 256, 0, s>>>(p);
+  } else {
+    const uint32_t rb = (6 * p.C + kReduceThreads - 1) / kReduceThreads;
+    if (p.shared) k_product_reduce<true><<<rb, kReduceThreads, 0, s>>>(p);
+    else k_product_reduce<false><<<rb, kReduceThreads, 0, s>>>(p);
+  }
   k_pcg_update<<<(p.m + kUpdateRows - 1) / kUpdateRows, kUpdateThreads, 0, s>>>(p);
-  k_pcg_direction<<<(p.m + 255) / 256, 256, 0, s>>>(p);
+  k_pcg_direction<<<(p.C + 1 + 255) / 256, 256, 0, s>>>(p);
 }
 void launch_update_cameras(const Params& p, cudaStream_t s) { k_update_cameras<<<1, 256, 0, s>>>(p); }
 void launch_update_points(const Params& p, cudaStream_t s) {

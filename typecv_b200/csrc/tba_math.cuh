@@ -175,6 +175,103 @@ __host__ __device__ inline void move_pose(const double p[12], const double delta
   }
 }
 
+// The factors of one observation's Jacobian.  With the camera-frame point q, the projection's
+// derivative rows du, dv (d pixel / d q), the focal column jf = pixel - principal point, the
+// residual r and the Huber weight w, every product the solver needs is a few dozen FMAs (R the
+// camera rotation, delta = (omega, v) a camera step, g a 2-vector):
+//   J_c delta = [du . (omega x q + v), dv . (omega x q + v)]
+//   J_c^T g   = [q x h ; h]            with h = g_u du + g_v dv
+//   J_p y     = [du . (R y), dv . (R y)]
+//   J_p^T g   = R^T (g_u du + g_v dv)
+// so the Schur blocks W_i = w J_c^T J_p never need to be stored: they are recomputed from the
+// pose, the camera, the point and the pixel.  A bearing has no translation columns; a fixed
+// camera has no J_c.
+struct Geo {
+  double q[3], du[3], dv[3], jf[2], r[2], w, sq;
+};
+
+// radial_limit(k1, k2) is a per-camera constant; `limit` passes it in.
+__host__ __device__ inline bool geometry(const double pose[12], const Camera& k, double limit, const double X[3],
+                                         bool directional, double u, double v, double huber, Geo& g) {
+  for (int i = 0; i < 3; i++) {
+    g.q[i] = pose[i * 3] * X[0] + pose[i * 3 + 1] * X[1] + pose[i * 3 + 2] * X[2];
+    if (!directional) g.q[i] += pose[9 + i];
+  }
+  if (!(g.q[2] > 1e-12)) return false;
+  const double iz = 1.0 / g.q[2];
+  const double x = g.q[0] * iz, y = g.q[1] * iz, r2 = x * x + y * y;
+  if (!(r2 < limit && r2 < 1e8)) return false;
+  const double d = 1 + k.k1 * r2 + k.k2 * r2 * r2, gg = 2 * (k.k1 + 2 * k.k2 * r2);
+  if (!(d > 0 && 1 + 3 * k.k1 * r2 + 5 * k.k2 * r2 * r2 > 0)) return false;
+  const double xx = d + gg * x * x, xy = gg * x * y, yy = d + gg * y * y;
+  const double px = k.fx * x * d, py = k.fy * y * d;
+  g.du[0] = k.fx * xx * iz;
+  g.du[1] = k.fx * xy * iz;
+  g.du[2] = -k.fx * (xx * x + xy * y) * iz;
+  g.dv[0] = k.fy * xy * iz;
+  g.dv[1] = k.fy * yy * iz;
+  g.dv[2] = -k.fy * (xy * x + yy * y) * iz;
+  const double mp = fmax(fabs(px + k.cx), fabs(py + k.cy));
+  const double mu = fmax(fmax(fabs(g.du[0]), fabs(g.du[1])), fabs(g.du[2]));
+  const double mv = fmax(fmax(fabs(g.dv[0]), fabs(g.dv[1])), fabs(g.dv[2]));
+  if (!(mp < 1e12 && mu < 1e12 && mv < 1e12)) return false;
+  g.jf[0] = px;
+  g.jf[1] = py;
+  g.r[0] = (px + k.cx) - u;
+  g.r[1] = (py + k.cy) - v;
+  g.sq = g.r[0] * g.r[0] + g.r[1] * g.r[1];
+  g.w = g.sq > huber * huber ? huber / sqrt(g.sq) : 1.0;
+  return true;
+}
+
+// W_i^T x = w J_p^T (J_c x_c + jf x_f): the point-side product of one observation.
+__host__ __device__ inline void wt_product(const Geo& g, const double pose[12], const double* xc, double xf,
+                                           bool variable, bool directional, bool shared, double t[3]) {
+  double au = 0, av = 0;
+  if (variable) {
+    double m0 = xc[1] * g.q[2] - xc[2] * g.q[1];
+    double m1 = xc[2] * g.q[0] - xc[0] * g.q[2];
+    double m2 = xc[0] * g.q[1] - xc[1] * g.q[0];
+    if (!directional) {
+      m0 += xc[3];
+      m1 += xc[4];
+      m2 += xc[5];
+    }
+    au = g.du[0] * m0 + g.du[1] * m1 + g.du[2] * m2;
+    av = g.dv[0] * m0 + g.dv[1] * m1 + g.dv[2] * m2;
+  }
+  if (shared) {
+    au += g.jf[0] * xf;
+    av += g.jf[1] * xf;
+  }
+  au *= g.w;
+  av *= g.w;
+  const double h0 = au * g.du[0] + av * g.dv[0], h1 = au * g.du[1] + av * g.dv[1], h2 = au * g.du[2] + av * g.dv[2];
+  for (int c = 0; c < 3; c++) t[c] = pose[c] * h0 + pose[3 + c] * h1 + pose[6 + c] * h2;
+}
+
+// W_i y = w J_c^T (J_p y) (6, zero for a fixed camera) and the focal share w jf . (J_p y).
+__host__ __device__ inline void w_product(const Geo& g, const double pose[12], const double y[3], bool variable,
+                                          bool directional, double d[6], double& e) {
+  const double R0 = pose[0] * y[0] + pose[1] * y[1] + pose[2] * y[2];
+  const double R1 = pose[3] * y[0] + pose[4] * y[1] + pose[5] * y[2];
+  const double R2 = pose[6] * y[0] + pose[7] * y[1] + pose[8] * y[2];
+  const double bu = g.w * (g.du[0] * R0 + g.du[1] * R1 + g.du[2] * R2);
+  const double bv = g.w * (g.dv[0] * R0 + g.dv[1] * R1 + g.dv[2] * R2);
+  e = bu * g.jf[0] + bv * g.jf[1];
+  if (!variable) {
+    for (int c = 0; c < 6; c++) d[c] = 0;
+    return;
+  }
+  const double h0 = bu * g.du[0] + bv * g.dv[0], h1 = bu * g.du[1] + bv * g.dv[1], h2 = bu * g.du[2] + bv * g.dv[2];
+  d[0] = g.q[1] * h2 - g.q[2] * h1;
+  d[1] = g.q[2] * h0 - g.q[0] * h2;
+  d[2] = g.q[0] * h1 - g.q[1] * h0;
+  d[3] = directional ? 0.0 : h0;
+  d[4] = directional ? 0.0 : h1;
+  d[5] = directional ? 0.0 : h2;
+}
+
 // The linearisation of one observation: everything the point block, the camera block and the
 // Schur product need, from the pose, the camera, the point and the observed pixel.
 struct ObsLin {
