@@ -218,3 +218,38 @@ def test_helix_midsize_matches_operator_oracle(device):
         assert abs(out[base + 6] - ref[base + 6]) <= COST_REL * ref[base + 6]
         assert abs(out[base + 16] - ref[base + 16]) <= 2 * 6
         assert rep["lm_iterations"] >= 1
+
+
+MIXED_REL = 1e-6  # mixed form: final cost against the FP64 form and the FP64 oracle
+
+
+@pytest.mark.parametrize("kind", ["ring", "helix"])
+def test_mixed_precision_reaches_the_fp64_cost(device, kind):
+    # The mixed form (FP32 Jacobian factors and Schur product inside the FP64 LM loop; each PCG
+    # solution refined by its FP64 residual, and finished on the FP64 product when the FP32 run
+    # stops short) has no reference counterpart; it is held to the FP64 form and to the FP64
+    # oracle on the same inputs.
+    scene = S.ring_scene(seed=11) if kind == "ring" else S.helix_scene(cameras=40, points=4000)
+    s, i = scene.packed()
+    packed = {"C": scene.C, "P": scene.P, "M": scene.M, "scene": s, "index": i}
+    base = 12 * scene.C + 3 * scene.P
+    for shared in (True, False):
+        kw = dict(anchor=0, scale_view=1, iterations=10, shared_focal=shared, tolerance=1e-8, max_cg=200)
+        o64, _ = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, precision=0, **kw), s, i)
+        o32, rep = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, precision=1, **kw), s, i)
+        ref = ob.gpu_operator_packed(packed, 0, 1, iterations=10, huber=2.0, max_cg=200, tolerance=1e-8, shared=shared)
+        c64, c32, cr = o64[base + 6], o32[base + 6], ref[base + 6]
+        assert abs(c32 - c64) <= MIXED_REL * c64, (c32, c64)
+        assert abs(c32 - cr) <= MIXED_REL * cr, (c32, cr)
+        assert o32[base + 10] > 0 and o32[base + 17] == 0
+        assert np.max(np.abs(o32[:12 * scene.C] - o64[:12 * scene.C])) < 1e-5
+
+
+def test_mixed_precision_through_the_operator(device):
+    jf = joint_focal_fixture()
+    inp = jf["input"]
+    mixed = tb.bundle_adjust_gpu(device, inp, FOCAL, precision="mixed")
+    fp64 = tb.bundle_adjust_gpu(device, inp, FOCAL)
+    assert mixed["diagnostics"]["finalCost"] < 1e-7 and mixed["diagnostics"]["finalRmsePx"] < 1e-4
+    assert abs(mixed["reconstruction"]["views"][0]["camera"]["fx"] - jf["truth"]["views"][0]["camera"]["fx"]) < 0.001
+    assert abs(mixed["diagnostics"]["finalCost"] - fp64["diagnostics"]["finalCost"]) < 1e-7

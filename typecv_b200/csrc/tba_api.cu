@@ -173,10 +173,11 @@ Chunks build_chunks(const uint32_t* cs, uint32_t C, uint32_t M, int sms) {
   return ch;
 }
 
+// Reads the first 40 state words into the pinned buffer; returns word `word`.
 double read_word(tba_device* d, const double* state, int word) {
-  CUDA_TRY(cudaMemcpyAsync(d->pinned, state + word, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  CUDA_TRY(cudaMemcpyAsync(d->pinned, state, 40 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
   CUDA_TRY(cudaStreamSynchronize(d->stream));
-  return d->pinned[0];
+  return d->pinned[word];
 }
 
 cudaEvent_t event(tba_device* d, size_t k) {
@@ -216,6 +217,9 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.huber = ctl->huber;
   p.tol = ctl->cg_tolerance;
   p.stall = ctl->stall_tolerance;
+  // The mixed form's inner PCG runs stop at a relative residual the FP32 product can reach; the
+  // FP64 refinement then measures the true residual against the caller's tolerance.
+  p.tol_inner = ctl->precision == TBA_PRECISION_MIXED ? std::max(ctl->cg_tolerance, 1e-6) : ctl->cg_tolerance;
   p.ntasks = ntasks;
   p.nchunks = nchunks;
   p.task_blocks = std::max<uint32_t>(1, std::min<uint32_t>(4 * d->sms, (ntasks + 7) / 8));
@@ -343,33 +347,59 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   launches += 4;
   CUDA_TRY(cudaGetLastError());
   bool lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
+  tba::Params tail = p;
+  tail.factored = 0;
+  tail.F = nullptr;
+  tail.F32 = nullptr;
+  tail.tol_inner = 0;  // the tail stops at the solve's own tolerance
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
-    const size_t first_pair = product_events.size();
     tba::launch_point_pass(p, s);
     tba::launch_camera_pass(p, s);
     tba::launch_camera_finish(p, s);
     tba::launch_pcg_init(p, s);
     launches += 4;
-    uint32_t done = 0, chunk = 8;
-    while (done < ctl->max_cg) {
-      const uint32_t k = std::min(chunk, ctl->max_cg - done);
-      for (uint32_t j = 0; j < k; j++) {
-        if (time_products) {
-          const size_t e0 = ev++, e1 = ev++;
-          CUDA_TRY(cudaEventRecord(event(d, e0), s));
-          tba::launch_product(p, s);
-          CUDA_TRY(cudaEventRecord(event(d, e1), s));
-          product_events.emplace_back(e0, e1);
-        } else {
-          tba::launch_product(p, s);
+    // PCG in chunks of guarded iterations; the read after each chunk only ends the loop early.
+    uint32_t done = 0, steps_before = 0;
+    // `q` selects the product: the engine's own (FP32 factors in the mixed form), or the FP64
+    // two-pass product of the mixed form's tail.  Only the engine's own products are timed.
+    auto run_pcg = [&](uint32_t budget, const tba::Params& q, bool timed) {
+      const size_t first_pair = product_events.size();
+      uint32_t chunk = 8;
+      while (done < budget) {
+        const uint32_t k = std::min(chunk, budget - done);
+        for (uint32_t j = 0; j < k; j++) {
+          if (time_products && timed) {
+            const size_t e0 = ev++, e1 = ev++;
+            CUDA_TRY(cudaEventRecord(event(d, e0), s));
+            tba::launch_product(q, s);
+            CUDA_TRY(cudaEventRecord(event(d, e1), s));
+            product_events.emplace_back(e0, e1);
+          } else {
+            tba::launch_product(q, s);
+          }
+          tba::launch_product_finish(q, s);
+          launches += q.factored ? 5 : 6;
         }
-        tba::launch_product_finish(p, s);
-        launches += 5;
+        CUDA_TRY(cudaGetLastError());
+        done += k;
+        if (done >= budget || read_word(d, p.state, tba::S_CG_ACTIVE) == 0) break;
+        chunk = std::min<uint32_t>(2 * chunk, 32);
       }
+      // The products of this run that did PCG steps (later launches of a chunk are no-ops).
+      const uint32_t steps = uint32_t(read_word(d, p.state, tba::S_CG_SOLVE_STEPS));
+      if (time_products && timed) product_spans.emplace_back(first_pair, steps - steps_before);
+      steps_before = steps;
+    };
+    run_pcg(ctl->max_cg, p, true);
+    // Mixed form: FP64 iterative refinement.  The true residual of the FP32-product solution
+    // restarts the PCG when it is above the tolerance, and the restarted run (with an iteration
+    // budget of its own) uses the FP64 two-pass product, which resolves what FP32 factors cannot
+    // on badly conditioned systems.
+    if (mixed) {
+      tba::launch_refine(p, s);
+      launches += 4;
       CUDA_TRY(cudaGetLastError());
-      done += k;
-      if (done >= ctl->max_cg || read_word(d, p.state, tba::S_CG_ACTIVE) == 0) break;
-      chunk = std::min<uint32_t>(2 * chunk, 32);
+      if (read_word(d, p.state, tba::S_CG_ACTIVE) != 0) run_pcg(done + ctl->max_cg, tail, false);
     }
     tba::launch_update_cameras(p, s);
     tba::launch_update_points(p, s);
@@ -381,7 +411,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     CUDA_TRY(cudaMemcpyAsync(d->pinned, p.state, 32 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     lm_active = d->pinned[tba::S_ACTIVE] != 0;
-    product_spans.emplace_back(first_pair, uint32_t(d->pinned[tba::S_CG_SOLVE_STEPS]));
   }
   tba::launch_pack(p, s);
   launches++;

@@ -46,6 +46,9 @@ enum StateWord : int {
   S_POINT_FAILED = 31,     // a point block failed this LM iteration
   S_ALPHA = 32,            // step length of the current PCG iteration
   S_BETA = 33,             // direction update of the current PCG iteration
+  S_REFINE = 34,           // an FP64 refinement of the PCG solution is under way
+  S_REFINED = 35,          // refinements that restarted the PCG (this solve)
+  S_INNER_R0 = 36,         // residual^2 that the current inner PCG run is measured against
   S_WORDS = 64
 };
 
@@ -62,6 +65,7 @@ struct Params {
   uint32_t C, P, M, D, m;  // cameras, points, observations, directional points, unknowns
   uint32_t anchor, scale_view, normalize_scale, shared;
   double huber, tol, stall;
+  double tol_inner;  // PCG tolerance of one inner run (tol in FP64; looser in the mixed form)
   // scene (current) and candidate
   double* poses;    // 12C
   double* points;   // 3P
@@ -97,6 +101,7 @@ struct Params {
   float* F32;          // the same factors in FP32 (mixed precision), or null
   uint32_t Mpad;       // stride of a factor component
   uint32_t factored;   // 1: one-pass product over stored factors; 0: two-pass recompute
+  uint32_t refine;     // 1: this launch evaluates the FP64 product S x of the refinement
   uint32_t prod_blocks;  // grid of the one-pass product
   double* pw;          // 6C: the PCG direction of each camera in world axes (R^T omega, R^T v)
   double* xw;          // 6C: the PCG solution of each camera in world axes
@@ -132,6 +137,9 @@ void launch_product(const Params& p, cudaStream_t s);
 // One PCG step after the product: column reduction of the product partials and alpha, the
 // distributed update of x, r, z and beta, then the new direction p.
 void launch_product_finish(const Params& p, cudaStream_t s);
+// Mixed form: the FP64 residual r = b - S x of the PCG solution (the two-pass recompute product
+// on x), and the PCG restarted from it when it is above the tolerance.
+void launch_refine(const Params& p, cudaStream_t s);
 void launch_update_cameras(const Params& p, cudaStream_t s);
 void launch_update_points(const Params& p, cudaStream_t s);
 void launch_accept(const Params& p, cudaStream_t s);

@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(1024) k_pcg_init(Params P) {
   block_sum(v, red);
   if (threadIdx.x == 0) {
     st[S_RHO] = v[0];
-    st[S_R0] = st[S_R2] = v[1];
+    st[S_R0] = st[S_R2] = st[S_INNER_R0] = v[1];
     if (v[1] > 0 && v[0] > 0) st[S_CG_ACTIVE] = 1;
     else if (v[1] > 1e-24) st[S_CG_FAILED] = 1;
   }
@@ -590,9 +590,14 @@ __device__ inline void schur_point_finish(const Params& P, uint32_t pt, const do
   y[1] = make_double2(vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2], 0);
 }
 
+// The two-pass product runs while the PCG is active, or, with P.refine, on the refinement's x.
+__device__ inline bool product_idle(const Params& P) {
+  return P.refine ? P.state[S_REFINE] == 0 : P.state[S_CG_ACTIVE] == 0;
+}
+
 template <bool SHARED>
 __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_schur_points(Params P) {
-  if (P.state[S_CG_ACTIVE] == 0) return;
+  if (product_idle(P)) return;
   const double fscale = focal_scale(P, P.state[S_LOG_FOCAL]);
   const double pf = SHARED ? P.p[P.m - 1] : 0.0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -632,7 +637,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_schur_p
 template <bool SHARED>
 __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur_cameras(Params P) {
   __shared__ double red[7 * (kCameraThreads / 32)];
-  if (P.state[S_CG_ACTIVE] == 0) return;
+  if (product_idle(P)) return;
   const uint32_t ch = blockIdx.x, c = P.chunk_cam[ch];
   const bool variable = P.active[c] != 0;
   double v[7] = {0, 0, 0, 0, 0, 0, 0};  // sum_i W_i y (6), focal share (1)
@@ -999,7 +1004,9 @@ __global__ void __launch_bounds__(kUpdateThreads) k_pcg_update(Params P) {
   st[S_CG_STEPS] += 1;
   st[S_CG_SOLVE_STEPS] += 1;
   st[S_R2] = residual;
-  if (residual <= P.tol * P.tol * st[S_R0]) {
+  // An inner run ends at the solve's tolerance, or (mixed form) once it has reduced its own starting
+  // residual as far as its FP32 product resolves; the FP64 refinement then takes over.
+  if (residual <= fmax(P.tol * P.tol * st[S_R0], P.tol_inner * P.tol_inner * st[S_INNER_R0])) {
     st[S_CG_ACTIVE] = 0;
     st[S_CG_CONVERGED] = 1;
   } else if (!(rho > 0)) {
@@ -1024,6 +1031,104 @@ __global__ void k_pcg_direction(Params P) {
     to_world(P.poses + 12 * size_t(c), v, P.pw + 6 * size_t(c));
   } else if (c == P.C && P.shared) {
     P.p[P.m - 1] = P.z[P.m - 1] + beta * P.p[P.m - 1];
+  }
+}
+
+// ---- Mixed form: FP64 iterative refinement of the PCG solution ----------------------------------
+//
+// After the PCG ran on the FP32-factor product, k_refine_begin marks the refinement, the two-pass
+// FP64 recompute product evaluates S x (launched with p := x), and k_refine forms the true residual
+// r = b - S x, z = M^-1 r, p = z, rho and r.r.  Its last block adds the focal row and either accepts
+// x (r.r within the tolerance: the PCG stays finished) or restarts the PCG from x with this r.
+
+__global__ void k_refine_begin(Params P) {
+  double* st = P.state;
+  st[S_REFINE] = (st[S_ACTIVE] != 0 && st[S_CG_FAILED] == 0 && st[S_R0] > 0) ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
+  __shared__ double rs[kUpdateRows];
+  __shared__ double red[4 * (kUpdateThreads / 32)];
+  double* st = P.state;
+  if (st[S_REFINE] == 0) return;
+  const uint32_t n = 6 * P.C;
+  const uint32_t row = blockIdx.x * kUpdateRows + threadIdx.x;
+  const bool mine = threadIdx.x < uint32_t(kUpdateRows) && row < n;
+  double rr = 0;
+  double v[4] = {0, 0, 0, 0};  // r.r, r.z (camera rows), H_cf . x, observation share of the focal row
+  if (mine) {
+    const uint32_t c = row / 6, j = row % 6;
+    double sum = 0;
+    for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum += P.chunk_prod[8 * size_t(ch) + j];
+    const double* U = P.camU + 21 * size_t(c);
+    const double* xc = P.x + 6 * size_t(c);
+    double ux = 0;
+    for (int k = 0; k < 6; k++) ux += U[sym6(j, k)] * xc[k];
+    double sx = ux - sum;
+    if (P.shared) {
+      sx += P.camHcf[row] * P.x[P.m - 1];
+      v[2] = P.camHcf[row] * xc[j];
+    }
+    rr = P.camRhs[row] - sx;
+    P.r[row] = rr;
+    rs[threadIdx.x] = rr;
+  }
+  if (P.shared)
+    for (uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x; ch < P.nchunks; ch += gridDim.x * blockDim.x)
+      v[3] += P.chunk_prod[8 * size_t(ch) + 6];
+  __syncthreads();
+  if (mine) {
+    const uint32_t jr = row % 6, base = threadIdx.x - jr;
+    const double* Mi = P.camMinv + 36 * size_t(row / 6) + 6 * jr;
+    const double zz = Mi[0] * rs[base] + Mi[1] * rs[base + 1] + Mi[2] * rs[base + 2] + Mi[3] * rs[base + 3] +
+                      Mi[4] * rs[base + 4] + Mi[5] * rs[base + 5];
+    P.z[row] = zz;
+    P.p[row] = zz;
+    v[0] = rr * rr;
+    v[1] = rr * zz;
+  }
+  __syncthreads();
+  if (threadIdx.x < uint32_t(kUpdateRows / 6)) {
+    const uint32_t c = blockIdx.x * (kUpdateRows / 6) + threadIdx.x;
+    if (c < P.C) {
+      double pc[6];
+      for (int k = 0; k < 6; k++) pc[k] = P.p[6 * c + k];
+      to_world(P.poses + 12 * size_t(c), pc, P.pw + 6 * size_t(c));
+    }
+  }
+  block_sum(v, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) P.blk_part[4 * blockIdx.x + k] = v[k];
+  if (!last_block(P.ticket + 2)) return;
+  double t[4] = {0, 0, 0, 0};
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (int k = 0; k < 4; k++) t[k] += __ldcg(P.blk_part + 4 * b + k);
+  block_sum(t, red);
+  if (threadIdx.x != 0) return;
+  P.ticket[2] = 0;
+  double residual = t[0], rho = t[1];
+  if (P.shared) {
+    const double xf = P.x[n];
+    const double sxf = st[S_FOCAL_DIAG] * xf + t[2] - t[3];
+    const double rf = st[S_FOCAL_RHS] - sxf, zf = st[S_FOCAL_INV] * rf;
+    P.r[n] = rf;
+    P.z[n] = zf;
+    P.p[n] = zf;
+    residual += rf * rf;
+    rho += rf * zf;
+  }
+  st[S_REFINE] = 0;
+  st[S_R2] = residual;
+  if (residual <= P.tol * P.tol * st[S_R0]) {
+    st[S_CG_ACTIVE] = 0;
+    st[S_CG_CONVERGED] = 1;
+  } else if (rho > 0) {
+    st[S_RHO] = rho;
+    st[S_INNER_R0] = residual;
+    st[S_CG_ACTIVE] = 1;
+    st[S_REFINED] += 1;
+  } else {
+    st[S_CG_FAILED] = 1;  // no descent direction, or a residual that is not finite
   }
 }
 
@@ -1371,6 +1476,20 @@ void launch_product_finish(const Params& p, cudaStream_t s) {
   }
   k_pcg_update<<<(p.m + kUpdateRows - 1) / kUpdateRows, kUpdateThreads, 0, s>>>(p);
   k_pcg_direction<<<(p.C + 1 + 255) / 256, 256, 0, s>>>(p);
+}
+void launch_refine(const Params& p, cudaStream_t s) {
+  k_refine_begin<<<1, 1, 0, s>>>(p);
+  Params q = p;
+  q.refine = 1;
+  q.p = p.x;
+  if (p.shared) {
+    k_schur_points<true><<<p.task_blocks, kPointThreads, 0, s>>>(q);
+    k_schur_cameras<true><<<p.nchunks, kCameraThreads, 0, s>>>(q);
+  } else {
+    k_schur_points<false><<<p.task_blocks, kPointThreads, 0, s>>>(q);
+    k_schur_cameras<false><<<p.nchunks, kCameraThreads, 0, s>>>(q);
+  }
+  k_refine<<<(6 * p.C + kUpdateRows - 1) / kUpdateRows, kUpdateThreads, 0, s>>>(p);
 }
 void launch_update_cameras(const Params& p, cudaStream_t s) { k_update_cameras<<<1, 256, 0, s>>>(p); }
 void launch_update_points(const Params& p, cudaStream_t s) {
