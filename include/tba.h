@@ -45,8 +45,9 @@ typedef enum {
 /* Arithmetic of the solve.  TBA_PRECISION_FP64 is the drop-in (IEEE binary64 throughout).
  * TBA_PRECISION_MIXED stores the Jacobian factors and runs the Schur product in FP32 with FP64
  * accumulation, inside an FP64 LM loop (cost, gain, right-hand side and the camera/point block
- * inverses stay FP64) with one FP64 refinement of each PCG solution.  It has no reference
- * counterpart. */
+ * inverses stay FP64).  Each PCG solution is refined by its FP64 residual; when that residual is
+ * above the tolerance the PCG restarts from it on the FP64 product, with an iteration budget of
+ * its own.  It has no reference counterpart. */
 typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
 
 /* TBA_FLAG_TIME_PRODUCTS: bracket every Schur product with CUDA events and report their total
@@ -156,6 +157,72 @@ tba_status tba_bundle_adjust(tba_device* device, const tba_control* control, con
  */
 tba_status tba_scene_cost_noalloc(const tba_control* control, const double* scene, const uint32_t* index,
                                   double* result, void* stream, char* message, size_t message_len);
+
+/*
+ * Batched local-window bundle adjustment: many independent problems in one persistent launch
+ * (captured in a CUDA graph and replayed while the batch keeps its shape).  No counterpart in the
+ * reference, whose mapper runs one `bundleAdjustGpu` call per local window
+ * (src/sfm/mapper/mapper.ts:859-925 over the windows of src/sfm/bundle/local-bundle.ts:17-208);
+ * each problem here gets exactly the result record of tba_bundle_adjust on the same arrays and
+ * options (within rounding: the sums run in another order).
+ *
+ * Each problem is the reference's packed pair (scene, index) of tba_bundle_adjust, stored anywhere
+ * in the caller's `scene` and `index` arrays at the offsets its tba_batch_problem gives; its result
+ * record goes to `output` at output_offset (tba_output_size elements).  Problems may have at most
+ * tba_batch_max_cameras() cameras (their camera system lives in on-chip shared memory); bearings
+ * (directional points) are not supported here.
+ */
+typedef struct {
+  uint32_t cameras, points, observations;
+  uint32_t anchor, scale_view;
+  uint32_t reserved;      /* 0 */
+  uint64_t scene_offset;  /* first double of the problem's scene in `scene` */
+  uint64_t index_offset;  /* first word of the problem's index in `index` */
+  uint64_t output_offset; /* first double of the problem's result record in `output` */
+} tba_batch_problem;
+
+/* Options shared by every problem of a batch (tba_control's meaning).  `schedule` picks the
+ * launch shape: 0 lets the autotuner choose (timed trial launches the first time a batch shape is
+ * seen on the handle, cached afterwards), k >= 1 forces shape k - 1 of tba_batch_shape. */
+typedef struct {
+  uint32_t iterations;
+  uint32_t max_cg;
+  uint32_t shared_focal;
+  uint32_t precision;
+  uint32_t schedule;
+  uint32_t flags;
+  double huber;
+  double cg_tolerance;
+  double stall_tolerance;
+} tba_batch_control;
+
+typedef struct {
+  double solve_ms;     /* device time of the persistent launch (CUDA events) */
+  double upload_ms;    /* device time of the host-to-device copies */
+  double download_ms;  /* device time of the device-to-host copy */
+  double wall_ms;      /* host wall time of the call */
+  double tune_ms;      /* host wall time spent in autotuning trial launches (0 when cached) */
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  uint64_t lm_iterations; /* accepted + rejected steps, summed over the problems */
+  uint64_t cg_iterations; /* state word 16, summed over the problems */
+  uint32_t problems;
+  uint32_t schedule;      /* the launch shape used (0-based) */
+  uint32_t threads;       /* threads per block of that shape */
+  uint32_t blocks;        /* persistent blocks launched */
+  uint32_t graph_replayed; /* 1: the launch replayed a cached CUDA graph */
+  uint32_t kernel_launches;
+} tba_batch_report;
+
+/* The largest camera count of one batched problem, and the number of launch shapes. */
+uint32_t tba_batch_max_cameras(void);
+uint32_t tba_batch_shapes(void);
+/* Threads per block and compiled blocks per SM of launch shape k (0-based). */
+tba_status tba_batch_shape(uint32_t k, uint32_t* threads, uint32_t* min_blocks);
+
+tba_status tba_batch_adjust(tba_device* device, const tba_batch_control* control, const tba_batch_problem* problems,
+                            uint32_t count, const double* scene, size_t scene_len, const uint32_t* index,
+                            size_t index_len, double* output, size_t output_len, tba_batch_report* report);
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,8 @@ TBA_FLAG_TIME_PRODUCTS = 1
 
 # Every symbol include/tba.h declares.
 EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
-           "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc")
+           "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc", "tba_batch_max_cameras",
+           "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust")
 
 
 class LibraryError(RuntimeError):
@@ -42,6 +43,36 @@ class Report(ctypes.Structure):
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint32), ("lm_iterations", ctypes.c_uint32),
         ("cg_iterations", ctypes.c_uint32), ("product_launches", ctypes.c_uint32), ("engine", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class BatchProblem(ctypes.Structure):
+    _fields_ = [
+        ("cameras", ctypes.c_uint32), ("points", ctypes.c_uint32), ("observations", ctypes.c_uint32),
+        ("anchor", ctypes.c_uint32), ("scale_view", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("scene_offset", ctypes.c_uint64), ("index_offset", ctypes.c_uint64), ("output_offset", ctypes.c_uint64),
+    ]
+
+
+class BatchControl(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_uint32), ("max_cg", ctypes.c_uint32), ("shared_focal", ctypes.c_uint32),
+        ("precision", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+        ("huber", ctypes.c_double), ("cg_tolerance", ctypes.c_double), ("stall_tolerance", ctypes.c_double),
+    ]
+
+
+class BatchReport(ctypes.Structure):
+    _fields_ = [
+        ("solve_ms", ctypes.c_double), ("upload_ms", ctypes.c_double), ("download_ms", ctypes.c_double),
+        ("wall_ms", ctypes.c_double), ("tune_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+        ("lm_iterations", ctypes.c_uint64), ("cg_iterations", ctypes.c_uint64),
+        ("problems", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+        ("blocks", ctypes.c_uint32), ("graph_replayed", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -80,6 +111,16 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                       ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t, P(Report)]
     lib.tba_scene_cost_noalloc.restype = ctypes.c_int
     lib.tba_scene_cost_noalloc.argtypes = [P(Control), vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t]
+    lib.tba_batch_max_cameras.restype = ctypes.c_uint32
+    lib.tba_batch_max_cameras.argtypes = []
+    lib.tba_batch_shapes.restype = ctypes.c_uint32
+    lib.tba_batch_shapes.argtypes = []
+    lib.tba_batch_shape.restype = ctypes.c_int
+    lib.tba_batch_shape.argtypes = [ctypes.c_uint32, P(ctypes.c_uint32), P(ctypes.c_uint32)]
+    lib.tba_batch_adjust.restype = ctypes.c_int
+    lib.tba_batch_adjust.argtypes = [vp, P(BatchControl), P(BatchProblem), ctypes.c_uint32, P(ctypes.c_double),
+                                     ctypes.c_size_t, P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_double),
+                                     ctypes.c_size_t, P(BatchReport)]
     _lib = lib
     return lib
 

@@ -13,11 +13,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
 #include "../../include/tba.h"
+#include "tba_batch.cuh"
 #include "tba_engine.cuh"
 
 using tba::Params;
@@ -32,6 +35,13 @@ struct tba_device {
   size_t capacity = 0;
   double* pinned = nullptr;  // small host buffer for flag reads
   std::vector<cudaEvent_t> events;
+  // Batched solves: their own workspace, the cached graph of the last launch and its key, and
+  // the autotuner's choices by batch shape.
+  char* batch_arena = nullptr;
+  size_t batch_capacity = 0;
+  cudaGraphExec_t batch_graph = nullptr;
+  std::vector<char> batch_key;
+  std::map<std::string, int> tuned;
 };
 
 namespace {
@@ -452,6 +462,307 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   }
 }
 
+// ---- batched local-window solves ------------------------------------------------------------------
+
+// The caller's arrays of one batched problem, checked as tba_bundle_adjust checks a problem.
+tba_control batch_problem_control(const tba_batch_control* bc, const tba_batch_problem& q) {
+  tba_control c{};
+  c.cameras = q.cameras;
+  c.points = q.points;
+  c.directional_points = 0;
+  c.observations = q.observations;
+  c.anchor = q.anchor;
+  c.scale_view = q.scale_view;
+  c.iterations = bc->iterations;
+  c.max_cg = bc->max_cg;
+  c.shared_focal = bc->shared_focal;
+  c.precision = bc->precision;
+  c.flags = 0;
+  c.huber = bc->huber;
+  c.cg_tolerance = bc->cg_tolerance;
+  c.stall_tolerance = bc->stall_tolerance;
+  return c;
+}
+
+void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_problem* probs, uint32_t count,
+                 const double* scene, size_t scene_len, const uint32_t* index, size_t index_len, double* output,
+                 size_t output_len, tba_batch_report* report) {
+  const auto wall0 = std::chrono::steady_clock::now();
+  const bool shared = bc->shared_focal != 0, mixed = bc->precision == TBA_PRECISION_MIXED;
+  const uint32_t max_cams = tba::batch_max_cameras();
+  uint32_t Cmax = 2;
+  std::vector<uint32_t> tasks;
+  std::vector<uint64_t> task_first(count), task_count(count);
+  for (uint32_t k = 0; k < count; k++) {
+    const tba_batch_problem& q = probs[k];
+    const tba_control c = batch_problem_control(bc, q);
+    check_control(&c);
+    if (q.reserved != 0) argument("Invalid GPU BA batch: reserved field must be 0");
+    if (q.cameras > max_cams)
+      argument("Batched GPU BA problem has " + std::to_string(q.cameras) + " cameras; the block solver takes at most " +
+               std::to_string(max_cams));
+    if (uint64_t(3) * q.observations + q.points + 2ull * q.cameras + 2 > 0xffffffffull)
+      argument("GPU BA scene dimensions exceed integer index bounds");
+    if (q.scene_offset > scene_len || scene_len - q.scene_offset < tba_scene_size(&c))
+      argument("Invalid GPU BA batch: a scene lies outside the scene array");
+    if (q.index_offset > index_len || index_len - q.index_offset < tba_index_size(&c))
+      argument("Invalid GPU BA batch: an index lies outside the index array");
+    if (q.output_offset > output_len || output_len - q.output_offset < tba_output_size(&c))
+      argument("Invalid GPU BA batch: a result record lies outside the output array");
+    check_index(&c, index + q.index_offset);
+    check_scene(&c, scene + q.scene_offset, tba_scene_size(&c));
+    const std::vector<uint32_t> t = build_tasks(index + q.index_offset + 2 * size_t(q.observations), q.points);
+    task_first[k] = tasks.size();
+    task_count[k] = t.size() - 1;
+    tasks.insert(tasks.end(), t.begin(), t.end());
+    Cmax = std::max(Cmax, q.cameras);
+  }
+  // Result records must not overlap: the device writes each one whole.
+  std::vector<uint32_t> by_out(count);
+  std::iota(by_out.begin(), by_out.end(), 0u);
+  std::sort(by_out.begin(), by_out.end(), [&](uint32_t a, uint32_t b) { return probs[a].output_offset < probs[b].output_offset; });
+  for (uint32_t j = 1; j < count; j++) {
+    const tba_batch_problem& prev = probs[by_out[j - 1]];
+    const tba_control pc = batch_problem_control(bc, prev);
+    if (prev.output_offset + tba_output_size(&pc) > probs[by_out[j]].output_offset)
+      argument("Invalid GPU BA batch: result records overlap");
+  }
+  // Largest problems first (longest-processing-time order for the persistent blocks).
+  std::vector<uint32_t> order(count);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    return uint64_t(probs[a].observations) * probs[a].cameras > uint64_t(probs[b].observations) * probs[b].cameras;
+  });
+
+  // Device layout: the caller's arrays as they are, then the schedule and the workspace.
+  Layout L;
+  const size_t factor_size = mixed ? 4 : 8;
+  const size_t o_scene = L.take<double>(scene_len), o_index = L.take<uint32_t>(index_len),
+               o_out = L.take<double>(output_len), o_tasks = L.take<uint32_t>(tasks.size()),
+               o_desc = L.take<tba::BatchProblem>(count), o_order = L.take<uint32_t>(count),
+               o_queue = L.take<uint32_t>(4);
+  std::vector<size_t> o_tp(count), o_pb(count), o_F(count);
+  uint64_t M_total = 0;
+  for (uint32_t k = 0; k < count; k++) {
+    const tba_batch_problem& q = probs[k];
+    const size_t Mpad = (size_t(q.observations) + 31) / 32 * 32;
+    o_tp[k] = L.take<double>(3 * size_t(q.points));
+    o_pb[k] = L.take<double>(12 * size_t(q.points));
+    o_F[k] = L.take<char>(tba::kFactors * Mpad * factor_size);
+    M_total += q.observations;
+  }
+  if (d->batch_capacity < L.bytes) {
+    if (d->batch_graph) {
+      cudaGraphExecDestroy(d->batch_graph);
+      d->batch_graph = nullptr;
+      d->batch_key.clear();
+    }
+    if (d->batch_arena) CUDA_TRY(cudaFree(d->batch_arena));
+    d->batch_arena = nullptr;
+    d->batch_capacity = 0;
+    size_t free_bytes = 0, total_bytes = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_bytes, &total_bytes));
+    if (L.bytes > free_bytes)
+      throw Fail{TBA_ERROR_BUDGET, "GPU BA batch needs " + std::to_string(L.bytes) +
+                                       " bytes of device memory, more than the working budget of " +
+                                       std::to_string(free_bytes) + " bytes"};
+    CUDA_TRY(cudaMalloc(&d->batch_arena, L.bytes));
+    d->batch_capacity = L.bytes;
+  }
+  char* a = d->batch_arena;
+  const double* dscene = reinterpret_cast<const double*>(a + o_scene);
+  const uint32_t* dindex = reinterpret_cast<const uint32_t*>(a + o_index);
+  double* dout = reinterpret_cast<double*>(a + o_out);
+  const uint32_t* dtasks = reinterpret_cast<const uint32_t*>(a + o_tasks);
+  std::vector<tba::BatchProblem> desc(count);
+  for (uint32_t k = 0; k < count; k++) {
+    const tba_batch_problem& q = probs[k];
+    tba::BatchProblem& b = desc[k];
+    const uint32_t C = q.cameras, P = q.points, M = q.observations;
+    b.C = C;
+    b.P = P;
+    b.M = M;
+    b.ntasks = uint32_t(task_count[k]);
+    b.anchor = q.anchor;
+    b.scale_view = q.scale_view;
+    const uint32_t* act = index + q.index_offset + 3 * size_t(M) + P + C + 2;
+    uint32_t fixed = 0;
+    for (uint32_t c = 0; c < C; c++) fixed += act[c] == 0;
+    b.normalize_scale = fixed == 1;
+    b.Mpad = uint32_t((size_t(M) + 31) / 32 * 32);
+    const double* s = dscene + q.scene_offset;
+    b.poses0 = s;
+    b.points0 = s + 12 * size_t(C);
+    b.cams = s + 12 * size_t(C) + 3 * size_t(P);
+    b.pixels = s + 18 * size_t(C) + 3 * size_t(P);
+    const uint32_t* x = dindex + q.index_offset;
+    b.obs_camera = x;
+    b.obs_point = x + M;
+    b.point_start = x + 2 * size_t(M);
+    b.camera_start = b.point_start + P + 1;
+    b.camera_obs = b.camera_start + C + 1;
+    b.active = b.camera_obs + M;
+    b.tasks = dtasks + task_first[k];
+    b.tpoints = reinterpret_cast<double*>(a + o_tp[k]);
+    b.pblk = reinterpret_cast<double*>(a + o_pb[k]);
+    b.F = a + o_F[k];
+    b.output = dout + q.output_offset;
+    b.points = b.output + 12 * size_t(C);
+  }
+
+  tba::BatchArgs args{};
+  args.problems = reinterpret_cast<const tba::BatchProblem*>(a + o_desc);
+  args.order = reinterpret_cast<const uint32_t*>(a + o_order);
+  args.queue = reinterpret_cast<uint32_t*>(a + o_queue);
+  args.count = count;
+  args.Cmax = Cmax;
+  args.iterations = bc->iterations;
+  args.max_cg = bc->max_cg;
+  args.huber = bc->huber;
+  args.tol = bc->cg_tolerance;
+  args.tol_inner = mixed ? std::max(bc->cg_tolerance, 1e-6) : bc->cg_tolerance;
+  args.stall = bc->stall_tolerance;
+  const size_t smem = tba::batch_smem_bytes(Cmax);
+
+  cudaStream_t s = d->stream;
+  cudaEvent_t e0 = event(d, 0), e1 = event(d, 1), e2 = event(d, 2), e3 = event(d, 3);
+  uint64_t h2d = 0;
+  auto up = [&](size_t off, const void* src, size_t bytes) {
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(a + off, src, bytes, cudaMemcpyHostToDevice, s));
+    h2d += bytes;
+  };
+  CUDA_TRY(cudaEventRecord(e0, s));
+  up(o_scene, scene, scene_len * sizeof(double));
+  up(o_index, index, index_len * sizeof(uint32_t));
+  up(o_tasks, tasks.data(), tasks.size() * sizeof(uint32_t));
+  up(o_desc, desc.data(), desc.size() * sizeof(tba::BatchProblem));
+  up(o_order, order.data(), order.size() * sizeof(uint32_t));
+  CUDA_TRY(cudaEventRecord(e1, s));
+
+  auto blocks_of = [&](int shape) {
+    const int per_sm = tba::batch_blocks_per_sm(shape, shared, mixed, smem);
+    return std::min<int>(int(count), per_sm * d->sms);
+  };
+  // The launch shape: forced, cached, or tuned now by one timed LM iteration of the whole batch per
+  // shape (the trial launches write only the workspace and the device copy of the results).
+  double tune_ms = 0;
+  int shape = -1;
+  if (bc->schedule > 0) {
+    shape = int(bc->schedule) - 1;
+    if (shape >= tba::kBatchShapes) argument("Invalid GPU BA batch schedule");
+  } else {
+    int lg = 0;
+    while ((uint64_t(1) << (lg + 1)) <= std::max<uint64_t>(1, M_total)) lg++;
+    const std::string key = std::to_string(shared) + "/" + std::to_string(mixed) + "/" + std::to_string(Cmax) + "/" +
+                            std::to_string(lg) + "/" + std::to_string(count);
+    auto hit = d->tuned.find(key);
+    if (hit != d->tuned.end()) {
+      shape = hit->second;
+    } else {
+      const auto t0 = std::chrono::steady_clock::now();
+      float best = 0;
+      tba::BatchArgs trial = args;
+      trial.iterations = std::min<uint32_t>(args.iterations, 1);
+      cudaEvent_t ta = event(d, 4), tb = event(d, 5);
+      for (int k = 0; k < tba::kBatchShapes; k++) {
+        const int blocks = blocks_of(k);
+        if (blocks <= 0) continue;
+        CUDA_TRY(cudaMemsetAsync(trial.queue, 0, sizeof(uint32_t), s));
+        CUDA_TRY(cudaEventRecord(ta, s));
+        CUDA_TRY(tba::launch_batch(k, shared, mixed, trial, blocks, smem, s));
+        CUDA_TRY(cudaEventRecord(tb, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ta, tb));
+        if (shape < 0 || ms < best) {
+          best = ms;
+          shape = k;
+        }
+      }
+      if (shape < 0) throw Fail{TBA_ERROR_INTERNAL, "no launch shape of the batched solver fits the device"};
+      d->tuned[key] = shape;
+      tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+  const int blocks = blocks_of(shape);
+  if (blocks <= 0) throw Fail{TBA_ERROR_INTERNAL, "the batched solver's launch shape does not fit the device"};
+
+  // One persistent launch, captured once in a CUDA graph and replayed while its arguments stay.
+  std::vector<char> key(sizeof args + 3 * sizeof(int) + sizeof(size_t));
+  {
+    const int ints[3] = {shape, blocks, int(shared) | (int(mixed) << 1)};
+    std::memcpy(key.data(), &args, sizeof args);
+    std::memcpy(key.data() + sizeof args, ints, sizeof ints);
+    std::memcpy(key.data() + sizeof args + sizeof ints, &smem, sizeof smem);
+  }
+  bool replayed = true;
+  if (!d->batch_graph || d->batch_key != key) {
+    replayed = false;
+    if (d->batch_graph) {
+      CUDA_TRY(cudaGraphExecDestroy(d->batch_graph));
+      d->batch_graph = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e1c = cudaMemsetAsync(args.queue, 0, sizeof(uint32_t), s);
+    cudaError_t e2c = e1c == cudaSuccess ? tba::launch_batch(shape, shared, mixed, args, blocks, smem, s) : e1c;
+    cudaError_t e3c = cudaStreamEndCapture(s, &graph);
+    CUDA_TRY(e2c);
+    CUDA_TRY(e3c);
+    cudaError_t ei = cudaGraphInstantiate(&d->batch_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    CUDA_TRY(ei);
+    d->batch_key = key;
+  }
+  CUDA_TRY(cudaGraphLaunch(d->batch_graph, s));
+  CUDA_TRY(cudaEventRecord(e2, s));
+  // Download the result records, merged into contiguous runs.
+  uint64_t d2h = 0;
+  for (uint32_t j = 0; j < count;) {
+    const tba_batch_problem& q0 = probs[by_out[j]];
+    const size_t begin = q0.output_offset;
+    tba_control c0 = batch_problem_control(bc, q0);
+    size_t end = begin + tba_output_size(&c0);
+    uint32_t k = j + 1;
+    while (k < count && probs[by_out[k]].output_offset == end) {
+      const tba_control ck = batch_problem_control(bc, probs[by_out[k]]);
+      end += tba_output_size(&ck);
+      k++;
+    }
+    CUDA_TRY(cudaMemcpyAsync(output + begin, dout + begin, (end - begin) * sizeof(double), cudaMemcpyDeviceToHost, s));
+    d2h += (end - begin) * sizeof(double);
+    j = k;
+  }
+  CUDA_TRY(cudaEventRecord(e3, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (report) {
+    std::memset(report, 0, sizeof *report);
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    report->upload_ms = ms;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e1, e2));
+    report->solve_ms = ms;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e2, e3));
+    report->download_ms = ms;
+    report->tune_ms = tune_ms;
+    report->h2d_bytes = h2d;
+    report->d2h_bytes = d2h;
+    for (uint32_t k = 0; k < count; k++) {
+      const tba_batch_problem& q = probs[k];
+      const double* st = output + q.output_offset + 12 * size_t(q.cameras) + 3 * size_t(q.points);
+      report->lm_iterations += uint64_t(st[tba::S_ACCEPTED] + st[tba::S_REJECTED]);
+      report->cg_iterations += uint64_t(st[tba::S_CG_STEPS]);
+    }
+    report->problems = count;
+    report->schedule = uint32_t(shape);
+    report->threads = uint32_t(tba::batch_shape(shape).threads);
+    report->blocks = uint32_t(blocks);
+    report->graph_replayed = replayed ? 1 : 0;
+    report->kernel_launches = 2;
+    report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -491,6 +802,7 @@ tba_status tba_device_open(int ordinal, tba_device** out) {
     CUDA_TRY(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMallocHost(&d->pinned, 64 * sizeof(double)));
     CUDA_TRY(tba::configure_kernels());
+    CUDA_TRY(tba::batch_configure());
   } catch (const Fail& f) {
     g_open_error = f.message;
     tba_device_close(d);
@@ -505,6 +817,8 @@ void tba_device_close(tba_device* d) {
   cudaSetDevice(d->ordinal);
   if (d->stream) cudaStreamSynchronize(d->stream);
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
+  if (d->batch_graph) cudaGraphExecDestroy(d->batch_graph);
+  if (d->batch_arena) cudaFree(d->batch_arena);
   if (d->arena) cudaFree(d->arena);
   if (d->pinned) cudaFreeHost(d->pinned);
   if (d->stream) cudaStreamDestroy(d->stream);
@@ -531,6 +845,39 @@ tba_status tba_bundle_adjust(tba_device* d, const tba_control* control, const do
     check_scene(control, scene, scene_len);
     CUDA_TRY(cudaSetDevice(d->ordinal));
     solve(d, control, scene, index, output, report);
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
+  } catch (const std::exception& e) {
+    d->error = e.what();
+    return TBA_ERROR_INTERNAL;
+  }
+  return TBA_OK;
+}
+
+uint32_t tba_batch_max_cameras(void) { return tba::batch_max_cameras(); }
+uint32_t tba_batch_shapes(void) { return uint32_t(tba::kBatchShapes); }
+
+tba_status tba_batch_shape(uint32_t k, uint32_t* threads, uint32_t* min_blocks) {
+  if (k >= uint32_t(tba::kBatchShapes)) return TBA_ERROR_ARGUMENT;
+  const tba::BatchShape s = tba::batch_shape(int(k));
+  if (threads) *threads = uint32_t(s.threads);
+  if (min_blocks) *min_blocks = uint32_t(s.min_blocks);
+  return TBA_OK;
+}
+
+tba_status tba_batch_adjust(tba_device* d, const tba_batch_control* control, const tba_batch_problem* problems,
+                            uint32_t count, const double* scene, size_t scene_len, const uint32_t* index,
+                            size_t index_len, double* output, size_t output_len, tba_batch_report* report) {
+  if (!d) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (!control) argument("Invalid GPU BA batch: no control block");
+    if (count == 0 || !problems) argument("Invalid GPU BA batch: no problems");
+    if (!scene || !index || !output) argument("Invalid GPU BA arrays: null pointer");
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    solve_batch(d, control, problems, count, scene, scene_len, index, index_len, output, output_len, report);
   } catch (const Fail& f) {
     d->error = f.message;
     return f.status;

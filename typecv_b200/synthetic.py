@@ -12,6 +12,8 @@ camera record (fx, fy, cx, cy, k1, k2; src/contracts/camera-record.ts:12-38).
                     each point kept in a uniform 3-12 of the cameras that see it (configs 1, 4).
 * ``sphere_scene``  cameras on a jittered sphere facing its centre, points from a mixture of
                     Gaussians in a ball, geometric track lengths (config 2).
+* ``arc_scene``     a local window: cameras on an arc of the ring facing the origin, tracks of
+                    2-10 of the nearest cameras (``batch_scenes``: the 512 windows of config 3).
 
 Every scene then gets Gaussian pixel noise, uniform in-image outliers and a perturbed
 initialisation (rotation by an axis-angle of fixed size, translation by a fraction of its norm,
@@ -274,6 +276,34 @@ def _tracks(rng, poses, cams, X, track, width, height, geometric, mean=6.0, cand
     remap = np.cumsum(keep) - 1
     sel = keep[op]
     return oc[sel], remap[op[sel]], keep
+
+
+def arc_scene(seed=0, cameras=20, points=5000, radius=5.0, cube=2.0, spacing=np.pi / 24, track=(2, 10),
+              **kw) -> Scene:
+    """A local window of configuration 3: cameras evenly on an arc of the 5 m ring of
+    configuration 0 (7.5 degrees apart) facing the origin, points uniform in a 2 m cube, each kept
+    in a uniform 2-10 of the nearest cameras that see it."""
+    rng = np.random.default_rng(seed)
+    ang = spacing * (np.arange(cameras) - (cameras - 1) / 2)
+    centers = np.stack([radius * np.cos(ang), radius * np.sin(ang), np.zeros(cameras)], axis=1)
+    poses = poses_from(look_at(centers, np.zeros_like(centers)), centers)
+    cams = intrinsics(cameras)
+    X = rng.uniform(-cube / 2, cube / 2, size=(points, 3))
+    oc, op, keep = _tracks(rng, poses, cams, X, track, 1024, 768, geometric=False)
+    X = X[keep]
+    options = {"iterations": 10, "huberPx": 2.0, "cgRelativeTolerance": 1e-6, "refineSharedFocal": False}
+    return finish(f"arc-{cameras}x{points}", rng, poses, cams, X, oc, op, width=1024, height=768,
+                  options={**options, **kw.pop("options", {})}, **kw)
+
+
+def batch_scenes(seed=3, count=512, cameras=(5, 40), points=(500, 20_000), track=(2, 10)) -> list[Scene]:
+    """Configuration 3: `count` independent arc windows, camera counts uniform in 5-40, point
+    counts log-uniform in 500-20,000, each drawn from its own sub-seed."""
+    rng = np.random.default_rng(seed)
+    Cs = rng.integers(cameras[0], cameras[1] + 1, size=count)
+    Ps = np.rint(np.exp(rng.uniform(np.log(points[0]), np.log(points[1]), size=count))).astype(int)
+    subs = rng.integers(0, 2**31 - 1, size=count)
+    return [arc_scene(int(s), int(c), int(p), track=track) for s, c, p in zip(subs, Cs, Ps)]
 
 
 CONFIGS = {
