@@ -224,6 +224,62 @@ tba_status tba_batch_adjust(tba_device* device, const tba_batch_control* control
                             uint32_t count, const double* scene, size_t scene_len, const uint32_t* index,
                             size_t index_len, double* output, size_t output_len, tba_batch_report* report);
 
+/*
+ * The adjoint of a converged bundle adjustment: the vector-Jacobian product of the solution
+ * (poses and points) with respect to the observed pixels and two shared intrinsics, by implicit
+ * differentiation.  No counterpart in the reference.
+ *
+ * At the solution theta* the robust cost's gradient F vanishes in every free direction, so
+ * d theta* = -H^-1 (F_y dy + F_kappa d kappa), H the exact Hessian of the robust cost (second
+ * derivatives of the projection and of the Huber loss included).  The gauge is the solver's: the
+ * fixed cameras do not move and, with exactly one fixed camera, the anchor-to-scale-camera
+ * baseline keeps its value (the cost's scale invariance is removed by that constraint, not by H).
+ * The intrinsics are fixed inputs of the solve (refineSharedFocal off): kappa = (s, k1), where s
+ * scales every camera's fx and fy by exp(s) and k1 is added to every camera's k1; both
+ * derivatives are taken at s = 0 and the given k1.
+ *
+ * scene, index: the layouts of tba_bundle_adjust; the scene's poses and points are the
+ *   evaluation point (normally the output of a converged tba_bundle_adjust).
+ * control->newton_steps Newton iterations with the exact Hessian are taken from that point first
+ *   (the solver's own update and gauge normalisation; the system H + mu G, G the Gauss-Newton
+ *   matrix with the solver's IRLS weights, mu adapted by the robust cost of each candidate and
+ *   zero once steps are accepted at mu < 1e-6), to drive
+ *   the gradient to zero; with pixels changed slightly from those of a solution, they also re-solve
+ *   the perturbed problem (finite-difference checks).
+ * cotangent: 12C + 3P doubles on the output poses (R row-major, t) and points, or NULL (Newton
+ *   steps only).  pixels_bar: 2M doubles, d<cotangent, theta*>/d pixel.  intrinsics_bar: 2 doubles,
+ *   d/ds and d/dk1.  solution: 12C + 3P doubles receiving the evaluation point, or NULL.
+ * Bearings (directional points) are not supported here.
+ */
+typedef struct {
+  uint32_t cameras, points, observations;
+  uint32_t anchor, scale_view;
+  uint32_t newton_steps;  /* Newton iterations, 0..50 */
+  uint32_t max_cg;        /* PCG iterations per linear solve, 1..100000 */
+  uint32_t flags;         /* 0 */
+  double huber;           /* as tba_control.huber */
+  double cg_tolerance;    /* relative PCG residual of every linear solve, 1e-15..1e-2 */
+} tba_vjp_control;
+
+typedef struct {
+  double solve_ms;              /* device time of the whole call (CUDA events) */
+  double wall_ms;
+  double gradient_norm_initial; /* |F| at the given point */
+  double gradient_norm_final;   /* |F| at the evaluation point (after the Newton steps) */
+  double adjoint_residual;      /* relative residual reached by the adjoint's PCG */
+  uint32_t cg_iterations;       /* over every linear solve */
+  uint32_t newton_steps;        /* Newton iterations accepted */
+  uint32_t failed;              /* bits: 1 a point block, 2 a camera block not positive definite;
+                                   4 a PCG broke down; 8 a PCG did not reach the tolerance */
+  uint32_t invalid;             /* observations outside the projection's domain at the evaluation point */
+  uint32_t point_failures;      /* point blocks that were not positive definite in the last solve */
+} tba_vjp_report;
+
+tba_status tba_bundle_vjp(tba_device* device, const tba_vjp_control* control, const double* scene, size_t scene_len,
+                          const uint32_t* index, size_t index_len, const double* cotangent, size_t cotangent_len,
+                          double* pixels_bar, size_t pixels_bar_len, double* intrinsics_bar, double* solution,
+                          size_t solution_len, tba_vjp_report* report);
+
 #ifdef __cplusplus
 }
 #endif

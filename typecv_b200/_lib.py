@@ -18,7 +18,7 @@ TBA_FLAG_TIME_PRODUCTS = 1
 # Every symbol include/tba.h declares.
 EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
            "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc", "tba_batch_max_cameras",
-           "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust")
+           "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust", "tba_bundle_vjp")
 
 
 class LibraryError(RuntimeError):
@@ -79,6 +79,28 @@ class BatchReport(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class VjpControl(ctypes.Structure):
+    _fields_ = [
+        ("cameras", ctypes.c_uint32), ("points", ctypes.c_uint32), ("observations", ctypes.c_uint32),
+        ("anchor", ctypes.c_uint32), ("scale_view", ctypes.c_uint32), ("newton_steps", ctypes.c_uint32),
+        ("max_cg", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+        ("huber", ctypes.c_double), ("cg_tolerance", ctypes.c_double),
+    ]
+
+
+class VjpReport(ctypes.Structure):
+    _fields_ = [
+        ("solve_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
+        ("gradient_norm_initial", ctypes.c_double), ("gradient_norm_final", ctypes.c_double),
+        ("adjoint_residual", ctypes.c_double),
+        ("cg_iterations", ctypes.c_uint32), ("newton_steps", ctypes.c_uint32), ("failed", ctypes.c_uint32),
+        ("invalid", ctypes.c_uint32), ("point_failures", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -121,6 +143,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tba_batch_adjust.argtypes = [vp, P(BatchControl), P(BatchProblem), ctypes.c_uint32, P(ctypes.c_double),
                                      ctypes.c_size_t, P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_double),
                                      ctypes.c_size_t, P(BatchReport)]
+    lib.tba_bundle_vjp.restype = ctypes.c_int
+    lib.tba_bundle_vjp.argtypes = [vp, P(VjpControl), P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_uint32),
+                                   ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_double),
+                                   ctypes.c_size_t, P(ctypes.c_double), P(ctypes.c_double), ctypes.c_size_t,
+                                   P(VjpReport)]
     _lib = lib
     return lib
 

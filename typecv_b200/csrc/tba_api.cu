@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/tba.h"
+#include "tba_adjoint.cuh"
 #include "tba_batch.cuh"
 #include "tba_engine.cuh"
 
@@ -763,6 +764,220 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
   }
 }
 
+// ---- the adjoint ---------------------------------------------------------------------------------
+
+void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, const uint32_t* index,
+               const double* cotangent, double* pixels_bar, double* intrinsics_bar, double* solution,
+               tba_vjp_report* report) {
+  const auto wall0 = std::chrono::steady_clock::now();
+  const uint32_t C = vc->cameras, P = vc->points, M = vc->observations;
+  const uint32_t* active = index + 3 * size_t(M) + P + C + 2;
+  uint32_t fixed = 0;
+  for (uint32_t c = 0; c < C; c++) fixed += active[c] == 0;
+  tba::AdjParams A{};
+  A.C = C;
+  A.P = P;
+  A.M = M;
+  A.anchor = vc->anchor;
+  A.scale_view = vc->scale_view;
+  A.normalize_scale = fixed == 1;
+  A.huber = vc->huber;
+  A.tol = vc->cg_tolerance;
+  Layout L;
+  const size_t o_poses = L.take<double>(12 * size_t(C)), o_points = L.take<double>(3 * size_t(P)),
+               o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
+               o_index = L.take<uint32_t>(3 * size_t(M) + P + 2 * size_t(C) + 2),
+               o_hcp = L.take<double>(18 * size_t(M)), o_hcc = L.take<double>(21 * size_t(M)),
+               o_hpp = L.take<double>(6 * size_t(M)), o_gc = L.take<double>(6 * size_t(M)),
+               o_gp = L.take<double>(3 * size_t(M)), o_vinv = L.take<double>(6 * size_t(P)),
+               o_bp = L.take<double>(3 * size_t(P)), o_lp = L.take<double>(3 * size_t(P)),
+               o_yp = L.take<double>(3 * size_t(P)), o_U = L.take<double>(21 * size_t(C)),
+               o_minv = L.take<double>(36 * size_t(C)), o_bc = L.take<double>(6 * size_t(C)),
+               o_vec = L.take<double>(5 * 6 * size_t(C)), o_cot = L.take<double>(6 * size_t(C) + 3 * size_t(P)),
+               o_gcot = L.take<double>(12 * size_t(C) + 3 * size_t(P)), o_ybar = L.take<double>(2 * size_t(M)),
+               o_state = L.take<double>(tba::A_WORDS), o_tposes = L.take<double>(12 * size_t(C)),
+               o_tpoints = L.take<double>(3 * size_t(P));
+  if (d->capacity < L.bytes) {
+    if (d->arena) CUDA_TRY(cudaFree(d->arena));
+    d->arena = nullptr;
+    d->capacity = 0;
+    size_t free_bytes = 0, total_bytes = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_bytes, &total_bytes));
+    if (L.bytes > free_bytes)
+      throw Fail{TBA_ERROR_BUDGET, "GPU BA adjoint needs " + std::to_string(L.bytes) +
+                                       " bytes of device memory, more than the working budget of " +
+                                       std::to_string(free_bytes) + " bytes"};
+    CUDA_TRY(cudaMalloc(&d->arena, L.bytes));
+    d->capacity = L.bytes;
+  }
+  char* a = d->arena;
+  auto D = [&](size_t off) { return reinterpret_cast<double*>(a + off); };
+  A.poses = D(o_poses);
+  A.points = D(o_points);
+  A.cams = D(o_cams);
+  A.pixels = D(o_pixels);
+  uint32_t* dindex = reinterpret_cast<uint32_t*>(a + o_index);
+  A.obs_camera = dindex;
+  A.obs_point = dindex + M;
+  A.point_start = dindex + 2 * size_t(M);
+  A.camera_start = A.point_start + P + 1;
+  A.camera_obs = A.camera_start + C + 1;
+  A.active = A.camera_obs + M;
+  A.Hcp = D(o_hcp);
+  A.Hcc = D(o_hcc);
+  A.Hpp = D(o_hpp);
+  A.gc = D(o_gc);
+  A.gp = D(o_gp);
+  A.Vinv = D(o_vinv);
+  A.bp = D(o_bp);
+  A.lp = D(o_lp);
+  A.yp = D(o_yp);
+  A.U = D(o_U);
+  A.Minv = D(o_minv);
+  A.bc = D(o_bc);
+  double* vec = D(o_vec);
+  A.x = vec;
+  A.r = vec + 6 * size_t(C);
+  A.p = vec + 12 * size_t(C);
+  A.z = vec + 18 * size_t(C);
+  A.Sp = vec + 24 * size_t(C);
+  A.cot = D(o_cot);
+  A.ybar = D(o_ybar);
+  A.state = D(o_state);
+  A.tposes = D(o_tposes);
+  A.tpoints = D(o_tpoints);
+  A.mu = 0;
+
+  cudaStream_t s = d->stream;
+  cudaEvent_t e0 = event(d, 0), e1 = event(d, 1);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  };
+  CUDA_TRY(cudaEventRecord(e0, s));
+  up(A.poses, scene, 12 * sizeof(double) * C);
+  up(A.points, scene + 12 * size_t(C), 3 * sizeof(double) * P);
+  up(const_cast<double*>(A.cams), scene + 12 * size_t(C) + 3 * size_t(P), 6 * sizeof(double) * C);
+  up(const_cast<double*>(A.pixels), scene + 18 * size_t(C) + 3 * size_t(P), 2 * sizeof(double) * M);
+  up(dindex, index, sizeof(uint32_t) * (3 * size_t(M) + P + 2 * size_t(C) + 2));
+  tba::adj_launch_init(A, s);
+  CUDA_TRY(cudaGetLastError());
+
+  auto read_state = [&]() {
+    CUDA_TRY(cudaMemcpyAsync(d->pinned, A.state, tba::A_WORDS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+  };
+  uint32_t cg_total = 0, failed = 0, point_failures = 0;
+  double last_residual = 0, gnorm_initial = -1, gnorm = 0;
+  // One linear solve (H + gauge term) z = rhs by Schur complement and PCG; z lands in x (cameras)
+  // and lp (points).  The assembly also measures |F|^2 at the current point.
+  auto linear_solve = [&](uint32_t mode, bool cotangent_ready) {
+    A.rhs_mode = mode;
+    if (!cotangent_ready) tba::adj_launch_reset(A, s);
+    tba::adj_launch_assemble(A, s);
+    tba::adj_launch_pcg_init(A, s);
+    CUDA_TRY(cudaGetLastError());
+    uint32_t done = 0;
+    while (done < vc->max_cg) {
+      const uint32_t k = std::min<uint32_t>(16, vc->max_cg - done);
+      for (uint32_t j = 0; j < k; j++) tba::adj_launch_pcg_step(A, s);
+      CUDA_TRY(cudaGetLastError());
+      done += k;
+      read_state();
+      if (d->pinned[tba::A_ACTIVE] == 0) break;
+    }
+    read_state();
+    const double* st = d->pinned;
+    cg_total += uint32_t(st[tba::A_STEPS]);
+    last_residual = st[tba::A_R0] > 0 ? std::sqrt(st[tba::A_R2] / st[tba::A_R0]) : 0;
+    gnorm = std::sqrt(st[tba::A_GNORM]);
+    if (gnorm_initial < 0) gnorm_initial = gnorm;
+    const bool converged = st[tba::A_R2] <= vc->cg_tolerance * vc->cg_tolerance * st[tba::A_R0] || st[tba::A_R0] == 0;
+    if (st[tba::A_POINT_FAILED] != 0) failed |= 1;
+    point_failures = uint32_t(st[tba::A_POINT_FAILED]);
+    if (st[tba::A_CAMERA_FAILED] != 0) failed |= 2;
+    if (st[tba::A_FAILED] != 0) failed |= 4;
+    if (!converged) failed |= 8;
+    tba::adj_launch_back_substitute(A, s);
+    CUDA_TRY(cudaGetLastError());
+    return st[tba::A_INVALID];
+  };
+  double invalid = 0;
+  // Newton steps on H + mu G (G the IRLS Gauss-Newton matrix): mu shrinks tenfold after a step the
+  // robust cost accepts and reaches 0 (exact Newton) below 1e-6, and grows tenfold after a rejected
+  // one.  Candidates within a relative 1e-14 of the current cost count as accepted.
+  if (vc->newton_steps > 0) {
+    tba::adj_launch_cost(A, s);
+    read_state();
+  }
+  double cost = d->pinned[tba::A_COST], mu = 1e-2;
+  uint32_t accepted = 0;
+  for (uint32_t k = 0; k < vc->newton_steps; k++) {
+    A.mu = mu;
+    invalid = linear_solve(0, false);
+    tba::adj_launch_newton_candidate(A, s);
+    CUDA_TRY(cudaGetLastError());
+    read_state();
+    const double cand = d->pinned[tba::A_COST];
+    const bool solved = (failed & 5) == 0;
+    failed &= ~uint32_t(13);  // a damped solve that failed is retried with more damping
+    if (solved && cand <= cost * (1 + 1e-14)) {
+      tba::adj_launch_newton_commit(A, s);
+      CUDA_TRY(cudaGetLastError());
+      cost = cand;
+      accepted++;
+      mu = mu < 1e-6 ? 0.0 : mu / 10;
+    } else {
+      mu = std::max(1e-6, mu * 10);
+    }
+  }
+  A.mu = 0;
+  if (cotangent) {
+    double* gcot = D(o_gcot);
+    up(gcot, cotangent, sizeof(double) * (12 * size_t(C) + 3 * size_t(P)));
+    tba::adj_launch_reset(A, s);
+    tba::adj_launch_cotangent(A, gcot, s);
+    CUDA_TRY(cudaGetLastError());
+    invalid = linear_solve(1, true);
+    tba::adj_launch_vjp(A, s);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(pixels_bar, A.ybar, 2 * sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+    read_state();
+    if (intrinsics_bar) {
+      intrinsics_bar[0] = d->pinned[tba::A_SBAR];
+      intrinsics_bar[1] = d->pinned[tba::A_KBAR];
+    }
+  } else if (vc->newton_steps > 0) {
+    // The gradient at the final point.
+    tba::adj_launch_reset(A, s);
+    A.rhs_mode = 0;
+    tba::adj_launch_assemble(A, s);
+    read_state();
+    gnorm = std::sqrt(d->pinned[tba::A_GNORM]);
+    invalid = d->pinned[tba::A_INVALID];
+  }
+  if (solution) {
+    CUDA_TRY(cudaMemcpyAsync(solution, A.poses, 12 * sizeof(double) * C, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(solution + 12 * size_t(C), A.points, 3 * sizeof(double) * P, cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(cudaEventRecord(e1, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (report) {
+    std::memset(report, 0, sizeof *report);
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    report->solve_ms = ms;
+    report->gradient_norm_initial = gnorm_initial < 0 ? gnorm : gnorm_initial;
+    report->gradient_norm_final = gnorm;
+    report->adjoint_residual = cotangent ? last_residual : 0;
+    report->cg_iterations = cg_total;
+    report->newton_steps = accepted;
+    report->failed = failed;
+    report->invalid = uint32_t(invalid);
+    report->point_failures = point_failures;
+    report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -878,6 +1093,56 @@ tba_status tba_batch_adjust(tba_device* d, const tba_batch_control* control, con
     if (!scene || !index || !output) argument("Invalid GPU BA arrays: null pointer");
     CUDA_TRY(cudaSetDevice(d->ordinal));
     solve_batch(d, control, problems, count, scene, scene_len, index, index_len, output, output_len, report);
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
+  } catch (const std::exception& e) {
+    d->error = e.what();
+    return TBA_ERROR_INTERNAL;
+  }
+  return TBA_OK;
+}
+
+tba_status tba_bundle_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, size_t scene_len,
+                          const uint32_t* index, size_t index_len, const double* cotangent, size_t cotangent_len,
+                          double* pixels_bar, size_t pixels_bar_len, double* intrinsics_bar, double* solution,
+                          size_t solution_len, tba_vjp_report* report) {
+  if (!d) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (!vc) argument("Invalid GPU BA adjoint: no control block");
+    tba_control c{};
+    c.cameras = vc->cameras;
+    c.points = vc->points;
+    c.observations = vc->observations;
+    c.anchor = vc->anchor;
+    c.scale_view = vc->scale_view;
+    c.iterations = 0;
+    c.max_cg = 1;
+    c.huber = vc->huber;
+    c.cg_tolerance = 1e-6;
+    c.stall_tolerance = 1e-9;
+    check_control(&c);
+    if (vc->newton_steps > 50 || vc->max_cg < 1 || vc->max_cg > 100000 || vc->flags != 0 ||
+        !(std::isfinite(vc->cg_tolerance) && vc->cg_tolerance >= 1e-15 && vc->cg_tolerance <= 1e-2))
+      argument("Invalid GPU BA adjoint options");
+    if (!scene || !index) argument("Invalid GPU BA arrays: null pointer");
+    if (scene_len != tba_scene_size(&c)) argument("Invalid GPU BA scene array length");
+    if (index_len != tba_index_size(&c)) argument("Invalid GPU BA index array length");
+    const size_t n_theta = 12 * size_t(c.cameras) + 3 * size_t(c.points);
+    if (cotangent && (cotangent_len != n_theta || !pixels_bar || pixels_bar_len < 2 * size_t(c.observations)))
+      argument("Invalid GPU BA adjoint arrays: the cotangent needs 12C + 3P values and pixels_bar 2M");
+    if (solution && solution_len < n_theta) argument("Invalid GPU BA adjoint arrays: solution needs 12C + 3P values");
+    if (cotangent)
+      for (size_t i = 0; i < n_theta; i++)
+        if (!std::isfinite(cotangent[i])) argument("Invalid GPU BA adjoint: the cotangent is not finite");
+    if (uint64_t(3) * c.observations + c.points + 2ull * c.cameras + 2 > 0xffffffffull)
+      argument("GPU BA scene dimensions exceed integer index bounds");
+    check_index(&c, index);
+    check_scene(&c, scene, scene_len);
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    solve_vjp(d, vc, scene, index, cotangent, pixels_bar, intrinsics_bar, solution, report);
   } catch (const Fail& f) {
     d->error = f.message;
     return f.status;
