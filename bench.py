@@ -1,14 +1,21 @@
 """Benchmark of the bundle-adjustment operator on B200 (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config cfg2] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config cfg2] [--precision both|fp64|mixed]
+                    [--impl ours|reference]
 
-A step is one bundle adjustment of the configuration's full synthetic scene (seeded; see
-typecv_b200/synthetic.py), ``--iterations`` LM iterations.  ``value`` is LM steps per second of the
-whole job, measured on the device with CUDA events (the library's solve time: inputs already in
-HBM), the max over ranks; ``e2e`` is the same metric through the public call
-(``tba_bundle_adjust`` with pinned host buffers: host checks, host-to-device copies, the solve and
-the device-to-host read inside the timed region).  The working set of configuration 2 (~1.5 GB)
-is larger than L2, so no flush is needed between steps.
+Configuration 2 (the default; 1,500 cameras / 1M points / ~6.2M observations): a step is one
+bundle adjustment of the full seeded synthetic scene (typecv_b200/synthetic.py), 10 LM iterations.
+``value`` is LM steps per second of the whole job in the mixed-precision form, measured on the device
+with CUDA events (the library's solve time: inputs already in HBM), the max over ranks; the same
+figures of the FP64 form, run on the same scene in the same process, are under ``fp64``, with the two
+forms' final costs.  ``e2e`` is the same metric through the public call (``tba_bundle_adjust`` with
+pinned host buffers: host checks, host-to-device copies, the solve and the device-to-host read inside
+the timed region).  The working set (~1.5 GB) is larger than the 126 MB L2, so no flush is needed.
+``roofline`` describes the dominant kernel, the one-pass Schur product, from CUDA-event pairs the
+library records around every product launch.
+
+``--config cfg3`` runs the batched local-window solve (512 arc windows, one persistent launch) and
+``--config cfg4`` the adjoint of a 200-camera / 50k-point solve; each prints its own line.
 
 Multi-GPU runs are replicas (the operator does not shard): each rank solves its own copy of the
 scene, no collective touches the data path, and ``scaling`` is "weak".
@@ -44,11 +51,13 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="cfg2", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--config", default="cfg2", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--iterations", type=int, default=None, help="LM iterations per step")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the configuration's points (profiling)")
+    ap.add_argument("--count", type=int, default=512, help="cfg3: problems in the batch")
+    ap.add_argument("--fd", type=int, default=256, help="cfg4: finite-difference coordinates")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -72,10 +81,12 @@ def workload(scene, config, iterations):
 def product_bytes(scene, shared, prod_blocks, factor_bytes=8):
     """Algorithmic DRAM bytes of one launch of the one-pass Schur product k_product_f: per
     observation its 12 stored Jacobian factors (8 B each in FP64, 4 B in the mixed form) and its
-    camera and point index (8 B); per point V_p^-1 (6 words) and its offset (4 B); the direction
-    vector p (m words) and the per-block partial rows (prod_blocks x m words, written)."""
+    camera and point index (8 B); per point V_p^-1 (6 words); per warp task its first observation
+    (4 B, about one task per 28 observations, counted per point here); the direction in world axes
+    (6C words) and the per-block partial rows (prod_blocks x m words, written by the product and
+    read by the column reduction)."""
     m = 6 * scene.C + (1 if shared else 0)
-    return scene.M * (12 * factor_bytes + 8) + scene.P * (6 * 8 + 4) + 8 * m + 8 * m * prod_blocks
+    return scene.M * (12 * factor_bytes + 8) + scene.P * (6 * 8 + 4) + 8 * 6 * scene.C + 2 * 8 * m * prod_blocks
 
 
 def two_pass_bytes(scene, shared):
@@ -140,18 +151,17 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def dram_traffic(scene, shared):
-    """Per-launch DRAM bytes of k_product from the committed ncu summary, scaled to this scene by
+def dram_traffic(scene, precision):
+    """Per-launch DRAM bytes of k_product_f from the committed ncu summary, scaled to this scene by
     its observations (the capture ran a smaller scene; traffic grows with the observations)."""
-    path = os.path.join(ROOT, "profiles", "k_product_traffic.json")
+    path = os.path.join(ROOT, "profiles", "k_product_f_traffic.json")
     try:
         d = json.load(open(path))
     except OSError:
         return None
-    key = "shared" if shared else "fixed"
-    if key not in d:
+    if precision not in d:
         return None
-    return d[key]["dram_bytes_per_observation"] * scene.M
+    return d[precision]["dram_bytes_per_observation"] * scene.M
 
 
 def cpu_baseline_run(scene, iterations=1):
@@ -210,10 +220,19 @@ def sum_over_ranks(world, value):
     return float(t.item())
 
 
+
+
+def finish_dist(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    scene = make_scene(args.config, args.scale)
+    cfg = args.config if args.config in ("cfg0", "cfg1", "cfg2") else "cfg2"
+    scene = make_scene(cfg, args.scale)
     for _ in range(args.warmup):
         cpu_baseline_run(scene, 1)
     times, ran = [], 0
@@ -227,39 +246,32 @@ def run_reference(args, world, rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": workload(scene, args.config, 1), "impl": "reference",
+            "config": workload(scene, cfg, 1), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"1 LM iteration of the full {args.config} scene per step (the reference "
+                             "sample": f"1 LM iteration of the full {cfg} scene per step (the reference "
                                        "operator's algorithm restated in C++, oracle/ba_oracle.cpp)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def main():
-    args = parse()
-    world, rank, local = init_dist(args)
-    if args.impl == "reference":
-        run_reference(args, world, rank)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
+def pinned_like(a, torch):
+    if a.dtype == np.uint32:
+        p = torch.empty(a.size, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    else:
+        p = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy()
+    p[:] = a
+    return p
+
+
+def time_form(args, world, local, scene, precision, iterations):
+    """Warm-up and timed solves of one form; returns (reports, wall times, output, clocks)."""
     import torch
     import typecv_b200 as tb
     from typecv_b200 import _lib
-
-    scene = make_scene(args.config, args.scale)
-    iterations = args.iterations or scene.options.get("iterations", 10)
-    shared = True
     s_np, i_np = scene.packed()
-    # pinned host buffers for the end-to-end path
-    s_pin = torch.empty(s_np.size, dtype=torch.float64, pin_memory=True).numpy()
-    i_pin = torch.empty(i_np.size, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-    s_pin[:] = s_np
-    i_pin[:] = i_np
-    precision = _lib.TBA_PRECISION_MIXED if args.precision == "mixed" else _lib.TBA_PRECISION_FP64
+    s_pin, i_pin = pinned_like(s_np, torch), pinned_like(i_np, torch)
     ctl = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, iterations=iterations,
-                          shared_focal=shared, huber=2.0, tolerance=1e-6, precision=precision,
+                          shared_focal=True, huber=2.0, tolerance=1e-6, precision=precision,
                           flags=_lib.TBA_FLAG_TIME_PRODUCTS)
     out = torch.empty(12 * scene.C + 3 * scene.P + 27, dtype=torch.float64, pin_memory=True).numpy()
     dev = tb.ShadeDevice.open(local)
@@ -278,57 +290,265 @@ def main():
         clk = clocks.summary()
     finally:
         dev.close()
+    return reports, walls, out.copy(), clk
+
+
+def form_summary(world, scene, reports, walls, out):
     solve_s = sum(r["solve_ms"] for r in reports) / 1000
     lm = sum(r["lm_iterations"] for r in reports)
     cg = sum(r["cg_iterations"] for r in reports)
     t_max = max_over_ranks(world, solve_s)
     lm_all = sum_over_ranks(world, lm)
     e2e_max = max_over_ranks(world, sum(walls))
+    cg_all = sum_over_ranks(world, cg)
     base = 12 * scene.C + 3 * scene.P
-    final_cost, final_rmse = float(out[base + 6]), float(out[base + 25])
-    if rank != 0:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
+    return {"value": lm_all / t_max, "e2e": lm_all / e2e_max, "t_max": t_max,
+            "pcg_iterations_per_s": cg_all / t_max, "final_cost": float(out[base + 6]),
+            "final_rmse_px": float(out[base + 25]), "lm_iterations": lm, "cg_iterations": cg,
+            "refinements": sum(r.get("refinements", 0) for r in reports)}
+
+
+def roofline(scene, reports, precision):
     pk, pk_kind = peaks()
     prod_ms = sum(r["product_ms"] for r in reports)
     prod_n = sum(r["product_launches"] for r in reports)
-    n_sms = torch.cuda.get_device_properties(local).multi_processor_count
-    prod_blocks = n_sms  # one 512-thread block per SM (the product kernel's occupancy)
-    bytes_launch = product_bytes(scene, shared, prod_blocks, 4 if args.precision == "mixed" else 8)
+    blocks = reports[-1].get("product_blocks", 0) or 1
+    bytes_launch = product_bytes(scene, True, blocks, 4 if precision == "mixed" else 8)
     t_launch = prod_ms / max(prod_n, 1) / 1000
     achieved = bytes_launch / t_launch / 1e9 if prod_n else None
-    traffic = dram_traffic(scene, shared)
+    kernel = "k_product_f<FP32 factors>" if precision == "mixed" else "k_product_f<FP64 factors>"
+    return {"bound": "hbm", "kernel": kernel + " (one-pass Schur product S p over the stored Jacobian factors)",
+            "achieved": achieved, "peak": pk["hbm_gbs"], "peak_kind": pk_kind, "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"] if achieved else None,
+            "traffic": dram_traffic(scene, precision), "algorithmic_bytes": bytes_launch,
+            "launch_ms": 1000 * t_launch, "launches": prod_n, "product_blocks": blocks,
+            "two_pass_equivalent_gbs": two_pass_bytes(scene, True) / t_launch / 1e9 if prod_n else None}
+
+
+def run_single(args, world, rank, local):
+    scene = make_scene(args.config, args.scale)
+    iterations = args.iterations or scene.options.get("iterations", 10)
+    from typecv_b200 import _lib
+    forms = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    results = {}
+    for form in forms:
+        prec = _lib.TBA_PRECISION_MIXED if form == "mixed" else _lib.TBA_PRECISION_FP64
+        reports, walls, out, clk = time_form(args, world, local, scene, prec, iterations)
+        results[form] = (reports, walls, out, clk, form_summary(world, scene, reports, walls, out))
+    if rank != 0:
+        return
+    head = forms[0]
+    reports, walls, out, clk, summ = results[head]
     line = {
-        "metric": METRIC, "value": lm_all / t_max, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "metric": METRIC, "value": summ["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * summ["t_max"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
         "data": "synthetic (seeded; typecv_b200/synthetic.py)",
-        "config": {**workload(scene, args.config, iterations), "precision": args.precision,
-                   "parallelism": f"replicas x{world}"},
-        "pcg_iterations_per_s": sum_over_ranks(world, cg) / t_max if world > 1 else cg / t_max,
-        "final_cost": final_cost, "final_rmse_px": final_rmse,
-        "e2e": {"value": lm_all / e2e_max, "unit": UNIT, "h2d_bytes_per_step": int(reports[-1]["h2d_bytes"]),
+        "config": {**workload(scene, args.config, iterations), "precision": head, "parallelism": f"replicas x{world}"},
+        "pcg_iterations_per_s": summ["pcg_iterations_per_s"],
+        "final_cost": summ["final_cost"], "final_rmse_px": summ["final_rmse_px"],
+        "e2e": {"value": summ["e2e"], "unit": UNIT, "h2d_bytes_per_step": int(reports[-1]["h2d_bytes"]),
                 "d2h_bytes_per_step": int(reports[-1]["d2h_bytes"])},
-        "roofline": {"bound": "hbm", "kernel": "k_product_f (one-pass Schur product S p over stored Jacobian factors)",
-                     "achieved": achieved, "peak": pk["hbm_gbs"], "peak_kind": pk_kind, "unit": "GB/s",
-                     "frac": achieved / pk["hbm_gbs"] if achieved else None,
-                     "traffic": traffic, "algorithmic_bytes": bytes_launch,
-                     "launch_ms": 1000 * t_launch, "launches": prod_n,
-                     "two_pass_equivalent_gbs": two_pass_bytes(scene, shared) / t_launch / 1e9 if prod_n else None},
+        "roofline": roofline(scene, reports, head),
         "clocks": clk,
         "gpu_launches": sum(r["kernel_launches"] for r in reports),
     }
+    if head == "mixed":
+        line["mixed"] = {"refinements": summ["refinements"], "cg_iterations": summ["cg_iterations"]}
+    if len(forms) == 2:
+        r64, _, _, clk64, s64 = results["fp64"]
+        line["fp64"] = {"value": s64["value"], "e2e": s64["e2e"], "pcg_iterations_per_s": s64["pcg_iterations_per_s"],
+                        "final_cost": s64["final_cost"], "final_rmse_px": s64["final_rmse_px"],
+                        "roofline": roofline(scene, r64, "fp64"), "clocks": clk64,
+                        "gpu_launches": sum(r["kernel_launches"] for r in r64)}
+        line["mixed_vs_fp64"] = {"lm_steps_ratio": summ["value"] / s64["value"],
+                                 "final_cost_rel_diff": abs(summ["final_cost"] - s64["final_cost"]) / s64["final_cost"]}
     if world == 1 and not args.no_cpu_baseline:
         dt, ran, threads = cpu_baseline_run(scene, 1)
         line["cpu_baseline"] = {"value": ran / dt, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"1 LM iteration of the full {args.config} scene, {dt:.1f} s (the "
                                           "reference operator's algorithm restated in C++, oracle/ba_oracle.cpp)"}
     print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+
+
+def run_batch(args, world, rank, local):
+    """Configuration 3: 512 arc windows (C 5-40, P log-uniform 500-20k, tracks 2-10), 10 LM
+    iterations each, one persistent launch per batch, against one grid-engine call per problem."""
+    import torch
+    import typecv_b200 as tb
+    from typecv_b200 import batch as B
+    from typecv_b200 import synthetic as S
+    scenes = S.batch_scenes(count=args.count)
+    probs = [B.PackedProblem(s.C, s.P, s.M, *s.packed(), s.anchor, s.scale_view) for s in scenes]
+    n_scene = sum(p.scene.size for p in probs)
+    n_index = sum(p.index.size for p in probs)
+    s_pin = torch.empty(n_scene, dtype=torch.float64, pin_memory=True).numpy()
+    i_pin = torch.empty(n_index, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    packed = B.pack_batch(probs, False, scene=s_pin, index=i_pin)
+    out = torch.empty(packed.output_len, dtype=torch.float64, pin_memory=True).numpy()
+    iterations, max_cg = 10, 256
+    dev = tb.ShadeDevice.open(local)
+    res = {}
+    try:
+        for prec in ("mixed", "fp64"):
+            tune = None
+            for _ in range(max(args.warmup, 1)):
+                _, rep = B.batch_adjust(dev, packed, iterations=iterations, precision=prec, max_cg=max_cg, output=out)
+                tune = tune or rep
+            reps, walls = [], []
+            barrier(world)
+            with Clocks(local) as clocks:
+                for _ in range(args.steps):
+                    t0 = time.perf_counter()
+                    recs, rep = B.batch_adjust(dev, packed, iterations=iterations, precision=prec, max_cg=max_cg,
+                                               output=out)
+                    walls.append(time.perf_counter() - t0)
+                    reps.append(rep)
+                barrier(world)
+            res[prec] = (reps, walls, [r.copy() for r in recs], clocks.summary(), tune)
+        seq_ms, seq = 0.0, []
+        for sc, p in zip(scenes, probs):
+            ctl = tb.make_control(sc.C, sc.P, sc.M, anchor=0, scale_view=1, iterations=iterations, max_cg=max_cg)
+            o, rep = tb.solve_packed(dev, ctl, p.scene, p.index)
+            seq_ms += rep["solve_ms"]
+            seq.append(o.copy())
+    finally:
+        dev.close()
+    reps, walls, recs, clk, tune = res["mixed"]
+    solve_s = max_over_ranks(world, sum(r["solve_ms"] for r in reps) / 1000)
+    lm = sum_over_ranks(world, sum(r["lm_iterations"] for r in reps))
+    wall_s = max_over_ranks(world, sum(walls))
+    if rank != 0:
+        return
+
+    def worst(records):
+        w = 0.0
+        for sc, a, b in zip(scenes, records, seq):
+            base = 12 * sc.C + 3 * sc.P
+            w = max(w, abs(a[base + 6] - b[base + 6]) / b[base + 6])
+        return w
+
+    r64 = res["fp64"][0]
+    lm_seq = sum(int(o[12 * s.C + 3 * s.P + 10] + o[12 * s.C + 3 * s.P + 11]) for s, o in zip(scenes, seq))
+    line = {"metric": "batched local-window BA: LM steps/s over the batch (one persistent launch)",
+            "value": lm / solve_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * solve_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"cfg3: {len(scenes)} arc windows, {sum(s.C for s in scenes)} cameras / "
+                                   f"{sum(s.P for s in scenes)} points / {sum(s.M for s in scenes)} observations in "
+                                   f"total, 10 LM iterations each, PCG tolerance 1e-6 (max 256), mixed precision",
+                       "l2": "working set larger than L2"},
+            "problems_per_s": world * len(scenes) * args.steps / solve_s,
+            "e2e": {"value": lm / wall_s, "unit": UNIT, "h2d_bytes_per_step": int(reps[-1]["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(reps[-1]["d2h_bytes"])},
+            "schedule": {"shape": reps[-1]["schedule"], "threads": reps[-1]["threads"], "blocks": reps[-1]["blocks"],
+                         "tune_ms": tune["tune_ms"], "graph_replayed": reps[-1]["graph_replayed"]},
+            "fp64_batch": {"value": sum(r["lm_iterations"] for r in r64) / (sum(r["solve_ms"] for r in r64) / 1000),
+                           "worst_cost_rel_vs_sequential": worst(res["fp64"][2])},
+            "mixed_worst_cost_rel_vs_sequential": worst(recs),
+            "sequential_fp64": {"value": lm_seq / (seq_ms / 1000), "solve_ms": seq_ms,
+                                "note": "the same problems, one tba_bundle_adjust call each (grid engine, FP64)"},
+            "clocks": clk, "gpu_launches": sum(r["kernel_launches"] for r in reps)}
+    line["speedup_vs_sequential_fp64"] = line["value"] / line["sequential_fp64"]["value"]
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, world, rank, local):
+    """Configuration 4: the vector-Jacobian product of the converged 200-camera / 50k-point solve
+    (configuration 1's generator), and its central-difference check on `--fd` pixel coordinates
+    (h = 1e-6 px) of the same configuration without outliers."""
+    import typecv_b200 as tb
+    from typecv_b200 import adjoint as AD
+    from typecv_b200 import synthetic as S
+
+    def solved(dev, sc):
+        s, i = sc.packed()
+        ctl = tb.make_control(sc.C, sc.P, sc.M, anchor=0, scale_view=1, iterations=30, shared_focal=True,
+                              tolerance=1e-10, max_cg=256)
+        out, _ = tb.solve_packed(dev, ctl, s, i)
+        n = 12 * sc.C + 3 * sc.P
+        s2 = s.copy()
+        s2[:n] = out[:n]
+        s2[n:n + 6 * sc.C].reshape(sc.C, 6)[:, :2] *= np.exp(out[n + 26])
+        return s2, i
+
+    dev = tb.ShadeDevice.open(local)
+    try:
+        sc = S.helix_scene(seed=24, cameras=200, points=50_000)
+        s, i = solved(dev, sc)
+        g = np.random.default_rng(6).normal(size=12 * sc.C + 3 * sc.P)
+        g /= np.linalg.norm(g)
+        for _ in range(max(args.warmup, 1)):
+            AD.bundle_vjp(dev, sc.C, sc.P, sc.M, s, i, g)
+        times, reps = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            _, _, _, rep = AD.bundle_vjp(dev, sc.C, sc.P, sc.M, s, i, g)
+            times.append(time.perf_counter() - t0)
+            reps.append(rep)
+        clean = S.helix_scene(seed=24, cameras=200, points=50_000, outlier_rate=0.0)
+        cs, ci = solved(dev, clean)
+        ybar, kbar, sol, rep_fd = AD.bundle_vjp(dev, clean.C, clean.P, clean.M, cs, ci, g, newton_steps=6,
+                                                want_solution=True)
+        base = cs.copy()
+        base[:sol.size] = sol
+        coords = np.random.default_rng(7).choice(2 * clean.M, args.fd, replace=False)
+        off = 18 * clean.C + 3 * clean.P
+        h = 1e-6
+        fd = np.zeros(coords.size)
+        t0 = time.perf_counter()
+        for n, k in enumerate(coords):
+            sp, sm = base.copy(), base.copy()
+            sp[off + k] += h
+            sm[off + k] -= h
+            tp, _ = AD.newton_solution(dev, clean.C, clean.P, clean.M, sp, ci, steps=2)
+            tm, _ = AD.newton_solution(dev, clean.C, clean.P, clean.M, sm, ci, steps=2)
+            fd[n] = g @ (tp - tm) / (2 * h)
+        fd_s = time.perf_counter() - t0
+    finally:
+        dev.close()
+    if rank != 0:
+        return
+    an = ybar.ravel()[coords]
+    scale = float(np.max(np.abs(an)))
+    err = np.abs(fd - an)
+    solve_ms = statistics.median(r["solve_ms"] for r in reps)
+    line = {"metric": "BA adjoint: vector-Jacobian products of the converged solve per second",
+            "value": 1000.0 / solve_ms, "unit": "vjp/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": solve_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"cfg4: {sc.C} cameras / {sc.P} points / {sc.M} observations (configuration 1's "
+                                   "generator), solved with the shared focal refined and then fixed; cotangent unit "
+                                   "random on poses and points; exact Hessian, PCG tolerance 1e-12"},
+            "e2e": {"value": args.steps / sum(times), "unit": "vjp/s",
+                    "h2d_bytes_per_step": int(s.nbytes + i.nbytes + g.nbytes), "d2h_bytes_per_step": 16 * sc.M + 16},
+            "adjoint_cg_iterations": reps[-1]["cg_iterations"], "adjoint_residual": reps[-1]["adjoint_residual"],
+            "gradient_norm_at_solution": reps[-1]["gradient_norm_initial"],
+            "point_regularized": reps[-1]["point_failures"], "failed_bits": reps[-1]["failed"],
+            "fd_check": {"coordinates": int(args.fd), "h_px": h, "scene": "same generator without the 3% outliers",
+                         "median_abs_err_over_max": float(np.median(err) / scale),
+                         "max_abs_err_over_max": float(np.max(err) / scale),
+                         "median_rel_err": float(np.median(err / np.maximum(np.abs(an), 1e-3 * scale))),
+                         "newton_gradient_norm": rep_fd["gradient_norm_final"],
+                         "vjp_ms_clean": rep_fd["solve_ms"], "seconds": fd_s},
+            "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = init_dist(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        elif args.config == "cfg3":
+            run_batch(args, world, rank, local)
+        elif args.config == "cfg4":
+            run_adjoint(args, world, rank, local)
+        else:
+            run_single(args, world, rank, local)
+    finally:
+        finish_dist(world)
 
 
 if __name__ == "__main__":

@@ -91,7 +91,11 @@ typedef struct {
   uint32_t lm_iterations;  /* LM iterations that ran */
   uint32_t cg_iterations;  /* PCG iterations that ran (state word 16) */
   uint32_t product_launches; /* Schur products timed in product_ms */
-  uint32_t engine;         /* 0: grid engine (one problem over the whole GPU) */
+  uint32_t engine;         /* 0: grid engine, one-pass product over stored factors;
+                              1: grid engine, two-pass recompute product (camera systems beyond
+                                 on-chip memory) */
+  uint32_t product_blocks; /* blocks of the one-pass product (each writes one partial row) */
+  uint32_t refinements;    /* mixed form: PCG restarts from the FP64 residual */
 } tba_report;
 
 /* Lengths, in elements, of the arrays of one problem (bundleArraySizes, bundle-host.ts:134-143):
@@ -269,10 +273,14 @@ typedef struct {
   double adjoint_residual;      /* relative residual reached by the adjoint's PCG */
   uint32_t cg_iterations;       /* over every linear solve */
   uint32_t newton_steps;        /* Newton iterations accepted */
-  uint32_t failed;              /* bits: 1 a point block, 2 a camera block not positive definite;
+  uint32_t failed;              /* bits: 1 a point block that no shift made definite, 2 a camera
+                                   block not positive definite;
                                    4 a PCG broke down; 8 a PCG did not reach the tolerance */
   uint32_t invalid;             /* observations outside the projection's domain at the evaluation point */
-  uint32_t point_failures;      /* point blocks that were not positive definite in the last solve */
+  uint32_t point_failures;      /* point blocks of the last solve that were not positive definite and
+                                   were shifted by the smallest power-of-ten multiple of their mean
+                                   diagonal that makes them definite (their derivatives are then
+                                   approximate: such points have a nearly flat robust cost) */
 } tba_vjp_report;
 
 tba_status tba_bundle_vjp(tba_device* device, const tba_vjp_control* control, const double* scene, size_t scene_len,

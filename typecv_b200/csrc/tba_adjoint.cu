@@ -248,11 +248,25 @@ __global__ void __launch_bounds__(256) k_adj_points(AdjParams A) {
       for (int j = 0; j < 3; j++) g[j] += A.gp[3 * size_t(i) + j];
     }
     gsq[0] += g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-    const double M9[9] = {V[0], V[1], V[2], V[1], V[3], V[4], V[2], V[4], V[5]};
+    double M9[9] = {V[0], V[1], V[2], V[1], V[3], V[4], V[2], V[4], V[5]};
     double inv[6];
     double* vi = A.Vinv + 6 * size_t(pt);
-    if (!inverse3_spd(M9, inv)) {
+    bool ok = inverse3_spd(M9, inv);
+    if (!ok) {
+      // Not positive definite (a point whose track is mostly beyond the Huber threshold has a nearly
+      // flat cost along some direction): shift by the smallest power-of-ten multiple of the mean
+      // diagonal that makes it definite, and count it.
       atomicAdd(A.state + A_POINT_FAILED, 1.0);
+      const double scale = fmax(fabs(V[0] + V[3] + V[5]) / 3, 1e-12);
+      for (double tau = 1e-8; tau <= 1e2 && !ok; tau *= 10) {
+        M9[0] = V[0] + tau * scale;
+        M9[4] = V[3] + tau * scale;
+        M9[8] = V[5] + tau * scale;
+        ok = inverse3_spd(M9, inv);
+      }
+    }
+    if (!ok) {
+      A.state[A_POINT_SINGULAR] = 1;
       for (int j = 0; j < 6; j++) vi[j] = 0;
     } else {
       for (int j = 0; j < 6; j++) vi[j] = inv[j];
@@ -352,7 +366,7 @@ __global__ void __launch_bounds__(1024) k_adj_pcg_init(AdjParams A) {
   __shared__ double red[64];
   double* st = A.state;
   const uint32_t m = 6 * A.C;
-  const bool fail = st[A_POINT_FAILED] != 0 || st[A_CAMERA_FAILED] != 0;
+  const bool fail = st[A_POINT_SINGULAR] != 0 || st[A_CAMERA_FAILED] != 0;
   for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
     A.r[j] = A.bc[j];
     A.x[j] = 0;
@@ -612,7 +626,8 @@ __global__ void k_adj_init(AdjParams A) {
 
 __global__ void k_adj_reset(AdjParams A) {
   const int w = threadIdx.x;
-  if (w == A_GNORM || w == A_INVALID || w == A_POINT_FAILED || w == A_CAMERA_FAILED || w == A_DOT || w == A_SBAR ||
+  if (w == A_GNORM || w == A_INVALID || w == A_POINT_FAILED || w == A_POINT_SINGULAR || w == A_CAMERA_FAILED ||
+      w == A_DOT || w == A_SBAR ||
       w == A_KBAR)
     A.state[w] = 0;
 }

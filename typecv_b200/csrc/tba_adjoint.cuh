@@ -32,7 +32,7 @@ namespace tba {
 enum AdjWord : int {
   A_RHO = 0, A_ALPHA = 1, A_BETA = 2, A_R0 = 3, A_R2 = 4, A_ACTIVE = 5, A_FAILED = 6, A_STEPS = 7,
   A_POINT_FAILED = 8, A_CAMERA_FAILED = 9, A_GNORM = 10, A_SBAR = 11, A_KBAR = 12, A_DOT = 13,
-  A_BASELINE = 14, A_ORIGIN = 15, A_SCALE = 18, A_INVALID = 19, A_COST = 20, A_WORDS = 32
+  A_BASELINE = 14, A_ORIGIN = 15, A_SCALE = 18, A_INVALID = 19, A_COST = 20, A_POINT_SINGULAR = 21, A_WORDS = 32
 };
 
 struct AdjParams {

@@ -250,7 +250,8 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
                o_tposes = L.take<double>(12 * size_t(C)), o_tpoints = L.take<double>(3 * size_t(P)),
                o_index = L.take<uint32_t>(3 * size_t(M) + P + 2 * size_t(C) + 2),
-               o_tasks = L.take<uint32_t>(tasks.size()), o_ccam = L.take<uint32_t>(nchunks),
+               o_tasks = L.take<uint32_t>(tasks.size()), o_tobs = L.take<uint32_t>(tasks.size()),
+               o_ccam = L.take<uint32_t>(nchunks),
                o_cbeg = L.take<uint32_t>(nchunks + 1), o_cfirst = L.take<uint32_t>(C + 1),
                o_rlim = L.take<double>(C), o_cmp = L.take<uint32_t>(M), o_cmx = L.take<double>(2 * size_t(M)),
                o_pblk = L.take<double>(12 * size_t(P)), o_y = L.take<double>(4 * size_t(P)),
@@ -294,6 +295,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.camera_obs = p.camera_start + C + 1;
   p.active = p.camera_obs + M;
   p.tasks = U32(o_tasks);
+  p.task_obs = U32(o_tobs);
   p.chunk_cam = U32(o_ccam);
   p.chunk_beg = U32(o_cbeg);
   p.cam_chunk = U32(o_cfirst);
@@ -341,12 +343,15 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   up(const_cast<double*>(p.pixels), scene + 18 * size_t(C) + 3 * size_t(P), 2 * sizeof(double) * M);
   up(dindex, index, sizeof(uint32_t) * (3 * size_t(M) + P + 2 * size_t(C) + 2));
   up(U32(o_tasks), tasks.data(), sizeof(uint32_t) * tasks.size());
+  std::vector<uint32_t> task_obs(tasks.size());
+  for (size_t t = 0; t < tasks.size(); t++) task_obs[t] = ps[tasks[t]];
+  up(U32(o_tobs), task_obs.data(), sizeof(uint32_t) * task_obs.size());
   up(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
   up(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
   up(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
   CUDA_TRY(cudaEventRecord(e_up, s));
 
-  uint32_t launches = 0, lm_done = 0;
+  uint32_t launches = 0, lm_done = 0, refinements = 0;
   // Event pairs around the Schur products; after the solve, only the products that ran PCG steps
   // (the first `steps` of each LM iteration; later ones are guarded no-ops) count.
   std::vector<std::pair<size_t, size_t>> product_events;
@@ -410,7 +415,10 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
       tba::launch_refine(p, s);
       launches += 4;
       CUDA_TRY(cudaGetLastError());
-      if (read_word(d, p.state, tba::S_CG_ACTIVE) != 0) run_pcg(done + ctl->max_cg, tail, false);
+      if (read_word(d, p.state, tba::S_CG_ACTIVE) != 0) {
+        refinements++;
+        run_pcg(done + ctl->max_cg, tail, false);
+      }
     }
     tba::launch_update_cameras(p, s);
     tba::launch_update_points(p, s);
@@ -458,7 +466,9 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     report->kernel_launches = launches;
     report->lm_iterations = lm_done;
     report->cg_iterations = uint32_t(output[12 * size_t(C) + 3 * size_t(P) + tba::S_CG_STEPS]);
-    report->engine = 0;
+    report->engine = p.factored ? 0 : 1;
+    report->product_blocks = p.factored ? p.prod_blocks : 0;
+    report->refinements = uint32_t(refinements);
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
   }
 }
@@ -892,7 +902,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     gnorm = std::sqrt(st[tba::A_GNORM]);
     if (gnorm_initial < 0) gnorm_initial = gnorm;
     const bool converged = st[tba::A_R2] <= vc->cg_tolerance * vc->cg_tolerance * st[tba::A_R0] || st[tba::A_R0] == 0;
-    if (st[tba::A_POINT_FAILED] != 0) failed |= 1;
+    if (st[tba::A_POINT_SINGULAR] != 0) failed |= 1;
     point_failures = uint32_t(st[tba::A_POINT_FAILED]);
     if (st[tba::A_CAMERA_FAILED] != 0) failed |= 2;
     if (st[tba::A_FAILED] != 0) failed |= 4;

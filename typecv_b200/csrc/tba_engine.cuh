@@ -81,7 +81,8 @@ struct Params {
   const uint32_t* camera_obs;
   const uint32_t* active;
   // schedules
-  const uint32_t* tasks;  // ntasks + 1 first points
+  const uint32_t* tasks;     // ntasks + 1 first points
+  const uint32_t* task_obs;  // ntasks + 1 first observations
   uint32_t ntasks;
   const uint32_t* chunk_cam;    // nchunks
   const uint32_t* chunk_beg;    // nchunks + 1 positions in camera_obs

@@ -620,48 +620,85 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
   double ef = 0;
   uint32_t tb, te;
   block_tasks(P, tb, te);
-  for (uint32_t t = tb + warp; t < te; t += nwarps) {
-    const uint32_t p0 = P.tasks[t], p1 = P.tasks[t + 1];
-    const uint32_t o0 = P.point_start[p0], n = P.point_start[p1] - o0;
-    const uint32_t rounds = n <= uint32_t(kTaskObs) ? 1 : (n + kTaskObs - 1) / kTaskObs;
-    // One point-aligned run of up to 32 observations per round; a long point takes several.
+  uint32_t t = tb + warp;
+  uint32_t o_next = t < te ? P.task_obs[t] : 0, e_next = t < te ? P.task_obs[t + 1] : 0;
+  for (; t < te; t += nwarps) {
+    const uint32_t o0 = o_next, n = e_next - o0;
+    if (t + nwarps < te) {  // the next task's bounds, early
+      o_next = P.task_obs[t + nwarps];
+      e_next = P.task_obs[t + nwarps + 1];
+    }
+    if (n <= uint32_t(kTaskObs)) {
+      // One observation per lane.  Every load the lane needs is issued before any arithmetic: its
+      // camera and point index, its factors, its point's V_p^-1 and its camera's direction.
+      const bool valid = uint32_t(lane) < n;
+      const uint32_t i = o0 + (valid ? lane : 0);
+      const uint32_t c = P.obs_camera[i], pt = P.obs_point[i];
+      Factors<T> f;
+      load_factors(FT, stride, i, f);
+      double vb[6], xw[6];
+      load6(P.pblk + 12 * size_t(pt), vb);
+      load6(P.pw + 6 * size_t(c), xw);
+      const bool variable = P.active[c] != 0;
+      const uint32_t p0 = __shfl_sync(kFull, pt, 0);
+      const int seg = valid ? int(pt - p0) : -1 - lane;
+      double s[3] = {0, 0, 0};
+      if (valid) factor_wt(f, xw, pf, variable, directional(P, pt), SHARED, s);
+      seg_scan(s, seg, lane);
+      const int next = __shfl_down_sync(kFull, seg, 1);
+      const bool tail = valid && (uint32_t(lane) == n - 1 || next != seg);
+      double y[3] = {0, 0, 0};
+      if (tail) {
+        y[0] = vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2];
+        y[1] = vb[1] * s[0] + vb[3] * s[1] + vb[4] * s[2];
+        y[2] = vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2];
+      }
+      const unsigned tails = __ballot_sync(kFull, tail);
+      const int src = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
+      for (int j = 0; j < 3; j++) y[j] = __shfl_sync(kFull, y[j], src);
+      if (!valid) continue;
+      const T y0 = T(y[0]), y1 = T(y[1]), y2 = T(y[2]);
+      const T gu = f.w * (f.ju[0] * y0 + f.ju[1] * y1 + f.ju[2] * y2);
+      const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
+      if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
+      if (!variable) continue;
+      const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
+      double* ac = acc + 6 * size_t(c);
+      atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
+      atomicAdd(ac + 1, -double(f.q[2] * h0 - f.q[0] * h2));
+      atomicAdd(ac + 2, -double(f.q[0] * h1 - f.q[1] * h0));
+      if (!directional(P, pt)) {
+        atomicAdd(ac + 3, -double(h0));
+        atomicAdd(ac + 4, -double(h1));
+        atomicAdd(ac + 5, -double(h2));
+      }
+      continue;
+    }
+    // A point with more than 32 observations: rounds of 32, one warp-wide sum.
+    const uint32_t p0 = P.obs_point[o0];
+    const uint32_t rounds = (n + kTaskObs - 1) / kTaskObs;
     double s[3] = {0, 0, 0};
-    int seg = -1 - lane;
-    uint32_t pt = 0;
     for (uint32_t r = 0; r < rounds; r++) {
       const uint32_t k = r * kTaskObs + lane;
       if (k < n) {
         const uint32_t i = o0 + k;
         const uint32_t c = P.obs_camera[i];
-        pt = P.obs_point[i];
-        seg = int(pt - p0);
         Factors<T> f;
         load_factors(FT, stride, i, f);
         double xw[6], u[3];
         load6(P.pw + 6 * size_t(c), xw);
-        factor_wt(f, xw, pf, P.active[c] != 0, directional(P, pt), SHARED, u);
+        factor_wt(f, xw, pf, P.active[c] != 0, directional(P, p0), SHARED, u);
         s[0] += u[0];
         s[1] += u[1];
         s[2] += u[2];
       }
     }
-    if (rounds == 1) seg_scan(s, seg, lane);
-    else warp_allsum(s);
-    const bool valid = uint32_t(lane) < n;
-    const int next = __shfl_down_sync(kFull, seg, 1);
-    const bool tail = rounds == 1 ? (valid && (uint32_t(lane) == n - 1 || next != seg)) : lane == 0;
-    double y[3] = {0, 0, 0};
-    if (tail) {
-      double vb[6];
-      load6(P.pblk + 12 * size_t(rounds == 1 ? pt : p0), vb);
-      y[0] = vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2];
-      y[1] = vb[1] * s[0] + vb[3] * s[1] + vb[4] * s[2];
-      y[2] = vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2];
-    }
-    const unsigned tails = __ballot_sync(kFull, tail);
-    const int src = rounds == 1 ? (valid ? __ffs(tails & (kFull << lane)) - 1 : lane) : 0;
-    for (int j = 0; j < 3; j++) y[j] = __shfl_sync(kFull, y[j], src);
-    const T y0 = T(y[0]), y1 = T(y[1]), y2 = T(y[2]);
+    warp_allsum(s);
+    double vb[6];
+    load6(P.pblk + 12 * size_t(p0), vb);
+    const T y0 = T(vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2]);
+    const T y1 = T(vb[1] * s[0] + vb[3] * s[1] + vb[4] * s[2]);
+    const T y2 = T(vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2]);
     for (uint32_t r = 0; r < rounds; r++) {
       const uint32_t k = r * kTaskObs + lane;
       if (k >= n) continue;
@@ -678,7 +715,7 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
       atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
       atomicAdd(ac + 1, -double(f.q[2] * h0 - f.q[0] * h2));
       atomicAdd(ac + 2, -double(f.q[0] * h1 - f.q[1] * h0));
-      if (!directional(P, P.obs_point[i])) {
+      if (!directional(P, p0)) {
         atomicAdd(ac + 3, -double(h0));
         atomicAdd(ac + 4, -double(h1));
         atomicAdd(ac + 5, -double(h2));
