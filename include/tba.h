@@ -83,7 +83,7 @@ typedef struct {
   double solve_ms;        /* device time from the first kernel to the last (CUDA events) */
   double upload_ms;       /* device time of the host-to-device copies */
   double download_ms;     /* device time of the device-to-host copy */
-  double wall_ms;         /* host wall time of the call */
+  double wall_ms;         /* host wall time of the call, after the structural checks */
   double product_ms;      /* device time of the Schur products alone (sampled by events) */
   uint64_t h2d_bytes;
   uint64_t d2h_bytes;
@@ -96,6 +96,7 @@ typedef struct {
                                  on-chip memory) */
   uint32_t product_blocks; /* blocks of the one-pass product (each writes one partial row) */
   uint32_t refinements;    /* mixed form: PCG restarts from the FP64 residual */
+  double check_ms;         /* host wall time of the structural checks of the arrays (before wall_ms) */
 } tba_report;
 
 /* Lengths, in elements, of the arrays of one problem (bundleArraySizes, bundle-host.ts:134-143):

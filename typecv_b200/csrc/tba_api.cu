@@ -17,6 +17,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/tba.h"
@@ -91,6 +92,41 @@ void check_control(const tba_control* c) {
 
 // The structure of the packed index array (bundleIndexLayout): every section consistent with the
 // others, so that no kernel can index out of bounds.
+// Runs f(begin, end, worker) over [0, n) split into up to `threads` contiguous ranges on host
+// threads (serially below `serial_below`).
+template <typename F>
+void parallel_ranges(uint64_t n, uint64_t serial_below, F f) {
+  unsigned threads = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (n < serial_below || threads == 1) {
+    f(uint64_t(0), n, 0u);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < threads; t++)
+    pool.emplace_back([&, t] { f(n * t / threads, n * (t + 1) / threads, t); });
+  for (auto& th : pool) th.join();
+}
+
+// The first failure over parallel ranges: the lowest position that failed, and its message.
+struct FirstFailure {
+  std::mutex mu;
+  uint64_t at = UINT64_MAX;
+  const char* message = nullptr;
+  void record(uint64_t where, const char* m) {
+    std::lock_guard<std::mutex> lock(mu);
+    if (where < at) {
+      at = where;
+      message = m;
+    }
+  }
+  void raise() const {
+    if (message) argument(message);
+  }
+};
+
+// The structure of the packed index array (bundleIndexLayout): every section consistent with the
+// others, so that no kernel can index out of bounds.  Large arrays are checked on host threads;
+// the failure reported is the one a serial scan in this order would meet first.
 void check_index(const tba_control* c, const uint32_t* index) {
   const uint64_t C = c->cameras, P = c->points, M = c->observations;
   const uint32_t* obs_camera = index;
@@ -100,24 +136,46 @@ void check_index(const tba_control* c, const uint32_t* index) {
   const uint32_t* cam_obs = cs + C + 1;
   const uint32_t* active = cam_obs + M;
   if (ps[0] != 0 || ps[P] != M) argument("Invalid GPU BA index: point offsets do not cover the observations");
-  for (uint64_t p = 0; p < P; p++) {
-    if (ps[p + 1] > M) argument("Invalid GPU BA index: point offsets exceed the observations");
-    if (ps[p + 1] < ps[p] + 2) argument("Landmarks require at least two observations");
-    for (uint64_t i = ps[p]; i < ps[p + 1]; i++)
-      if (obs_point[i] != p) argument("Invalid GPU BA index: observation point does not match the point offsets");
+  {
+    FirstFailure ff;
+    parallel_ranges(P, 1u << 16, [&](uint64_t b, uint64_t e, unsigned) {
+      for (uint64_t p = b; p < e; p++) {
+        if (ps[p + 1] > M) return ff.record(p, "Invalid GPU BA index: point offsets exceed the observations");
+        if (ps[p + 1] < ps[p] + 2) return ff.record(p, "Landmarks require at least two observations");
+        for (uint64_t i = ps[p]; i < ps[p + 1]; i++)
+          if (obs_point[i] != p)
+            return ff.record(p, "Invalid GPU BA index: observation point does not match the point offsets");
+      }
+    });
+    ff.raise();
   }
-  for (uint64_t i = 0; i < M; i++)
-    if (obs_camera[i] >= C) argument("Invalid GPU BA index: observation camera out of range");
+  {
+    FirstFailure ff;
+    parallel_ranges(M, 1u << 18, [&](uint64_t b, uint64_t e, unsigned) {
+      for (uint64_t i = b; i < e; i++)
+        if (obs_camera[i] >= C) return ff.record(i, "Invalid GPU BA index: observation camera out of range");
+    });
+    ff.raise();
+  }
   if (cs[0] != 0 || cs[C] != M) argument("Invalid GPU BA index: camera offsets do not cover the observations");
-  std::vector<uint8_t> seen(M, 0);
-  for (uint64_t cam = 0; cam < C; cam++) {
-    if (cs[cam + 1] < cs[cam] || cs[cam + 1] > M) argument("Invalid GPU BA index: camera offsets decrease or exceed the observations");
-    for (uint64_t k = cs[cam]; k < cs[cam + 1]; k++) {
-      const uint32_t i = cam_obs[k];
-      if (i >= M || seen[i] || obs_camera[i] != cam)
-        argument("Invalid GPU BA index: camera observation lists are not the observations of each camera");
-      seen[i] = 1;
-    }
+  for (uint64_t cam = 0; cam < C; cam++)
+    if (cs[cam + 1] < cs[cam] || cs[cam + 1] > M)
+      argument("Invalid GPU BA index: camera offsets decrease or exceed the observations");
+  {
+    // Each observation may be claimed only by its own camera, so a thread owning a range of
+    // cameras is the only one to touch `seen` for their observations.
+    std::vector<uint8_t> seen(M, 0);
+    FirstFailure ff;
+    parallel_ranges(C, M < (1u << 18) ? C + 1 : 1, [&](uint64_t b, uint64_t e, unsigned) {
+      for (uint64_t cam = b; cam < e; cam++)
+        for (uint64_t k = cs[cam]; k < cs[cam + 1]; k++) {
+          const uint32_t i = cam_obs[k];
+          if (i >= M || obs_camera[i] != cam || seen[i])
+            return ff.record(cam, "Invalid GPU BA index: camera observation lists are not the observations of each camera");
+          seen[i] = 1;
+        }
+    });
+    ff.raise();
   }
   uint32_t fixed = 0;
   for (uint64_t cam = 0; cam < C; cam++) {
@@ -130,11 +188,15 @@ void check_index(const tba_control* c, const uint32_t* index) {
 
 // finiteGpuArray and validateGpuCamera (src/geometry/gpu/bounds.ts:5-26) on the scene array.
 void check_scene(const tba_control* c, const double* scene, size_t len) {
-  for (size_t i = 0; i < len; i++) {
-    const double x = scene[i];
-    if (!std::isfinite(x) || std::fabs(x) > 1e9 || (x != 0 && std::fabs(x) < 1e-30))
-      argument("GPU BA input exceeds supported coordinate bounds");
-  }
+  FirstFailure ff;
+  parallel_ranges(len, 1u << 18, [&](uint64_t b, uint64_t e, unsigned) {
+    for (uint64_t i = b; i < e; i++) {
+      const double x = scene[i];
+      if (!std::isfinite(x) || std::fabs(x) > 1e9 || (x != 0 && std::fabs(x) < 1e-30))
+        return ff.record(i, "GPU BA input exceeds supported coordinate bounds");
+    }
+  });
+  ff.raise();
   const double* k = scene + 12 * size_t(c->cameras) + 3 * size_t(c->points);
   for (uint32_t cam = 0; cam < c->cameras; cam++, k += 6)
     if (!(k[0] > 0 && k[1] > 0) || k[0] < 1e-6 || k[1] < 1e-6 || k[0] > 1e6 || k[1] > 1e6 ||
@@ -1066,10 +1128,13 @@ tba_status tba_bundle_adjust(tba_device* d, const tba_control* control, const do
     if (output_len < tba_output_size(control)) argument("Invalid GPU BA output array length");
     if (uint64_t(3) * control->observations + control->points + 2ull * control->cameras + 2 > 0xffffffffull)
       argument("GPU BA scene dimensions exceed integer index bounds");
+    const auto t0 = std::chrono::steady_clock::now();
     check_index(control, index);
     check_scene(control, scene, scene_len);
+    const double check_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     CUDA_TRY(cudaSetDevice(d->ordinal));
     solve(d, control, scene, index, output, report);
+    if (report) report->check_ms = check_ms;
   } catch (const Fail& f) {
     d->error = f.message;
     return f.status;
