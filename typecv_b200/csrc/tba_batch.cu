@@ -268,9 +268,9 @@ __device__ __noinline__ void b_point_pass(const BatchProblem& Q, Sh& S) {
         seg = int(pt - p0);
         b_point_obs<SHARED, T>(Q, S, o0 + lane, pt, fscale, v, sc[0], sc[1]);
       }
-      seg_scan(v, seg, lane);
-      const int next = __shfl_down_sync(kFull, seg, 1);
-      if (uint32_t(lane) < n && (uint32_t(lane) == n - 1 || next != seg))
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(v, runs);
+      if (uint32_t(lane) < n && run_tail(runs, lane))
         b_point_finish<SHARED>(Q, S, pt, v, lambda, sc[2], sc[3]);
     } else {
       double v[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -524,11 +524,15 @@ __device__ __noinline__ void b_product_f(const BatchProblem& Q, Sh& S) {
         s[2] += u[2];
       }
     }
-    if (rounds == 1) seg_scan(s, seg, lane);
-    else warp_allsum(s);
+    Runs runs{0u, 0, 0};
+    if (rounds == 1) {
+      runs = lane_runs(seg, lane);
+      run_scan(s, runs);
+    } else {
+      warp_allsum(s);
+    }
     const bool valid = uint32_t(lane) < n;
-    const int next = __shfl_down_sync(kFull, seg, 1);
-    const bool tail = rounds == 1 ? (valid && (uint32_t(lane) == n - 1 || next != seg)) : lane == 0;
+    const bool tail = rounds == 1 ? (valid && run_tail(runs, lane)) : lane == 0;
     double y[3] = {0, 0, 0};
     if (tail) {
       const double* vb = Q.pblk + 12 * size_t(rounds == 1 ? pt : p0);
@@ -604,11 +608,15 @@ __device__ __noinline__ void b_product_r(const BatchProblem& Q, Sh& S, const dou
         }
       }
     }
-    if (rounds == 1) seg_scan(s, seg, lane);
-    else warp_allsum(s);
+    Runs runs{0u, 0, 0};
+    if (rounds == 1) {
+      runs = lane_runs(seg, lane);
+      run_scan(s, runs);
+    } else {
+      warp_allsum(s);
+    }
     const bool valid = uint32_t(lane) < n;
-    const int next = __shfl_down_sync(kFull, seg, 1);
-    const bool tail = rounds == 1 ? (valid && (uint32_t(lane) == n - 1 || next != seg)) : lane == 0;
+    const bool tail = rounds == 1 ? (valid && run_tail(runs, lane)) : lane == 0;
     double y[3] = {0, 0, 0};
     if (tail) {
       const double* vb = Q.pblk + 12 * size_t(rounds == 1 ? pt : p0);
@@ -948,9 +956,9 @@ __device__ __noinline__ void b_update_points(const BatchProblem& Q, Sh& S) {
           seg = int(pt - p0);
           b_update_wt<SHARED, T>(Q, S, i, Q.obs_camera[i], pt, fscale, xf, s);
         }
-        seg_scan(s, seg, lane);
-        const int next = __shfl_down_sync(kFull, seg, 1);
-        const bool tail = ok && (uint32_t(lane) == n - 1 || next != seg);
+        const Runs runs = lane_runs(seg, lane);
+        run_scan(s, runs);
+        const bool tail = ok && run_tail(runs, lane);
         double X[3] = {0, 0, 0};
         if (tail) b_candidate_point(Q, S, pt, s, X);
         const unsigned tails = __ballot_sync(kFull, tail);

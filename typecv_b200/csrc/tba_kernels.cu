@@ -265,9 +265,9 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
         seg = int(pt - p0);
         point_obs<SHARED>(P, o0 + lane, pt, fscale, v, sc[0], sc[1]);
       }
-      seg_scan(v, seg, lane);
-      const int next = __shfl_down_sync(kFull, seg, 1);
-      if (uint32_t(lane) < n && (uint32_t(lane) == n - 1 || next != seg))
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(v, runs);
+      if (uint32_t(lane) < n && run_tail(runs, lane))
         point_finish<SHARED>(P, pt, v, lambda, sc[2], sc[3]);
     } else {
       double v[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -544,9 +544,9 @@ __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_schur_p
         seg = int(pt - p0);
         schur_point_obs<SHARED>(P, o0 + lane, pt, fscale, pf, s);
       }
-      seg_scan(s, seg, lane);
-      const int next = __shfl_down_sync(kFull, seg, 1);
-      if (uint32_t(lane) < n && (uint32_t(lane) == n - 1 || next != seg)) schur_point_finish(P, pt, s);
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(s, runs);
+      if (uint32_t(lane) < n && run_tail(runs, lane)) schur_point_finish(P, pt, s);
     } else {
       double s[3] = {0, 0, 0};
       for (uint32_t base = 0; base < n; base += kTaskObs)
@@ -644,9 +644,9 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
       const int seg = valid ? int(pt - p0) : -1 - lane;
       double s[3] = {0, 0, 0};
       if (valid) factor_wt(f, xw, pf, variable, directional(P, pt), SHARED, s);
-      seg_scan(s, seg, lane);
-      const int next = __shfl_down_sync(kFull, seg, 1);
-      const bool tail = valid && (uint32_t(lane) == n - 1 || next != seg);
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(s, runs);
+      const bool tail = valid && run_tail(runs, lane);
       double y[3] = {0, 0, 0};
       if (tail) {
         y[0] = vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2];
@@ -1225,9 +1225,9 @@ __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_update_
         seg = int(pt - p0);
         update_wt(P, i, P.obs_camera[i], pt, fscale, xf, SHARED, s);
       }
-      seg_scan(s, seg, lane);
-      const int next = __shfl_down_sync(kFull, seg, 1);
-      const bool tail = valid && (uint32_t(lane) == n - 1 || next != seg);
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(s, runs);
+      const bool tail = valid && run_tail(runs, lane);
       double X[3] = {0, 0, 0};
       if (tail) candidate_point(P, pt, s, X);
       const unsigned tails = __ballot_sync(kFull, tail);

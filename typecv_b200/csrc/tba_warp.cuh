@@ -42,6 +42,38 @@ __device__ inline void seg_scan(double (&v)[N], int seg, int lane) {
   }
 }
 
+// Runs of equal `seg` over the lanes (contiguous): each lane's position in its run, the run heads
+// as a lane mask, and the largest position in the warp, which bounds the steps a scan needs.
+struct Runs {
+  unsigned heads;
+  int pos;
+  int maxpos;
+};
+
+__device__ inline Runs lane_runs(int seg, int lane) {
+  const int prev = __shfl_up_sync(kFull, seg, 1);
+  const unsigned heads = __ballot_sync(kFull, lane == 0 || prev != seg);
+  const int pos = lane - (31 - __clz(heads & (kFull >> (31 - lane))));
+  return Runs{heads, pos, int(__reduce_max_sync(kFull, unsigned(pos)))};
+}
+
+// Inclusive sum within each run, in as many doubling steps as the longest run needs.
+template <int N>
+__device__ inline void run_scan(double (&v)[N], const Runs& r) {
+  for (int d = 1; d <= r.maxpos; d <<= 1) {
+    double t[N];
+#pragma unroll
+    for (int n = 0; n < N; n++) t[n] = __shfl_up_sync(kFull, v[n], d);
+    if (r.pos >= d) {
+#pragma unroll
+      for (int n = 0; n < N; n++) v[n] += t[n];
+    }
+  }
+}
+
+// True in the last lane of each run.
+__device__ inline bool run_tail(const Runs& r, int lane) { return lane == 31 || ((r.heads >> (lane + 1)) & 1u); }
+
 template <int N>
 __device__ inline void warp_allsum(double (&v)[N]) {
 #pragma unroll
