@@ -55,6 +55,8 @@ enum StateWord : int {
 constexpr int kTaskObs = 32;        // observations per warp task (one per lane)
 constexpr int kFactors = 12;        // stored Jacobian factors per observation
 constexpr int kProductThreads = 384;  // two blocks per SM
+constexpr int kStagedThreads = 768;   // one block per SM, direction staged in shared memory
+constexpr int kStagedSmemLimit = 227 * 1024;
 
 constexpr int kPointThreads = 256;  // threads of the task kernels
 constexpr int kCameraThreads = 128;
@@ -152,6 +154,8 @@ uint32_t product_finish_blocks(const Params& p);
 // dynamic shared memory, the opt-in of the product kernels, and their blocks per SM.
 uint32_t product_max_unknowns();
 size_t product_smem_bytes(const Params& p);
+bool product_staged(const Params& p);
+int product_threads(const Params& p);
 cudaError_t configure_kernels();
 int product_blocks_per_sm(const Params& p);
 

@@ -606,12 +606,18 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // storage type: double for the FP64 form, float for the mixed form (the per-observation
 // arithmetic then runs in FP32 and every sum in FP64).
 
-template <bool SHARED, typename T>
-__global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
+// STAGED: the direction of every camera (world axes, 6C values of T) is staged in shared memory
+// after the camera sums, so the per-observation read of it is an on-chip gather; one block of
+// kStagedThreads per SM.  Otherwise it is read from global memory, two blocks of kProductThreads.
+template <bool SHARED, typename T, bool STAGED>
+__global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double acc[];
   if (P.state[S_CG_ACTIVE] == 0) return;
   const uint32_t m = P.m;
+  T* pws = reinterpret_cast<T*>(acc + ((m + 1) & ~1u));
   for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) acc[j] = 0;
+  if (STAGED)
+    for (uint32_t j = threadIdx.x; j < 6 * P.C; j += blockDim.x) pws[j] = T(P.pw[j]);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const T* FT = sizeof(T) == 4 ? reinterpret_cast<const T*>(P.F32) : reinterpret_cast<const T*>(P.F);
@@ -638,12 +644,16 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
       load_factors(FT, stride, i, f);
       double vb[6], xw[6];
       load6(P.pblk + 12 * size_t(pt), vb);
-      load6(P.pw + 6 * size_t(c), xw);
-      const bool variable = P.active[c] != 0;
+      if (STAGED)
+        for (int j = 0; j < 6; j++) xw[j] = double(pws[6 * c + j]);
+      else
+        load6(P.pw + 6 * size_t(c), xw);
+      // A fixed camera's direction is zero, so its observations add nothing on the camera side;
+      // their scatter lands in the fixed camera's rows, which k_product_columns discards.
       const uint32_t p0 = __shfl_sync(kFull, pt, 0);
       const int seg = valid ? int(pt - p0) : -1 - lane;
       double s[3] = {0, 0, 0};
-      if (valid) factor_wt(f, xw, pf, variable, directional(P, pt), SHARED, s);
+      if (valid) factor_wt(f, xw, pf, true, directional(P, pt), SHARED, s);
       const Runs runs = lane_runs(seg, lane);
       run_scan(s, runs);
       const bool tail = valid && run_tail(runs, lane);
@@ -661,7 +671,6 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
       const T gu = f.w * (f.ju[0] * y0 + f.ju[1] * y1 + f.ju[2] * y2);
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
-      if (!variable) continue;
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
       double* ac = acc + 6 * size_t(c);
       atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
@@ -686,8 +695,11 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
         Factors<T> f;
         load_factors(FT, stride, i, f);
         double xw[6], u[3];
-        load6(P.pw + 6 * size_t(c), xw);
-        factor_wt(f, xw, pf, P.active[c] != 0, directional(P, p0), SHARED, u);
+        if (STAGED)
+          for (int j = 0; j < 6; j++) xw[j] = double(pws[6 * c + j]);
+        else
+          load6(P.pw + 6 * size_t(c), xw);
+        factor_wt(f, xw, pf, true, directional(P, p0), SHARED, u);
         s[0] += u[0];
         s[1] += u[1];
         s[2] += u[2];
@@ -709,7 +721,6 @@ __global__ void __launch_bounds__(kProductThreads, 2) k_product_f(Params P) {
       const T gu = f.w * (f.ju[0] * y0 + f.ju[1] * y1 + f.ju[2] * y2);
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
-      if (P.active[c] == 0) continue;
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
       double* ac = acc + 6 * size_t(c);
       atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
@@ -768,7 +779,7 @@ __global__ void __launch_bounds__(256) k_product_columns(Params P) {
       double up = 0;
 #pragma unroll
       for (int k = 0; k < 6; k++) up += U[sym6(r, k)] * pc[k];
-      double sp = up + sum;
+      double sp = up + (P.active[c] != 0 ? sum : 0.0);  // a fixed camera's rows: U = I, p = 0
       if (SHARED) {
         sp += P.camHcf[j] * P.p[m - 1];
         v[1] = P.camHcf[j] * P.p[j];
@@ -1333,7 +1344,20 @@ uint32_t product_finish_blocks(const Params& p) {
 }
 
 uint32_t product_max_unknowns() { return (227 * 1024) / sizeof(double) - 64; }
-size_t product_smem_bytes(const Params& p) { return size_t(p.m) * sizeof(double); }
+
+// The direction is staged in shared memory when the camera sums and it fit one block.
+bool product_staged(const Params& p) {
+  const size_t word = p.F32 ? sizeof(float) : sizeof(double);
+  return size_t((p.m + 1) & ~1u) * sizeof(double) + 6 * size_t(p.C) * word <= size_t(kStagedSmemLimit);
+}
+
+size_t product_smem_bytes(const Params& p) {
+  const size_t word = p.F32 ? sizeof(float) : sizeof(double);
+  return product_staged(p) ? size_t((p.m + 1) & ~1u) * sizeof(double) + 6 * size_t(p.C) * word
+                           : size_t(p.m) * sizeof(double);
+}
+
+int product_threads(const Params& p) { return product_staged(p) ? kStagedThreads : kProductThreads; }
 
 cudaError_t configure_kernels() {
   const int bytes = 227 * 1024;
@@ -1341,18 +1365,25 @@ cudaError_t configure_kernels() {
   auto set = [&](const void* f) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   };
-  set(reinterpret_cast<const void*>(k_product_f<false, double>));
-  set(reinterpret_cast<const void*>(k_product_f<true, double>));
-  set(reinterpret_cast<const void*>(k_product_f<false, float>));
-  set(reinterpret_cast<const void*>(k_product_f<true, float>));
+  set(reinterpret_cast<const void*>(k_product_f<false, double, false>));
+  set(reinterpret_cast<const void*>(k_product_f<true, double, false>));
+  set(reinterpret_cast<const void*>(k_product_f<false, float, false>));
+  set(reinterpret_cast<const void*>(k_product_f<true, float, false>));
+  set(reinterpret_cast<const void*>(k_product_f<false, double, true>));
+  set(reinterpret_cast<const void*>(k_product_f<true, double, true>));
+  set(reinterpret_cast<const void*>(k_product_f<false, float, true>));
+  set(reinterpret_cast<const void*>(k_product_f<true, float, true>));
   return e;
 }
 
 int product_blocks_per_sm(const Params& p) {
   int n = 0;
-  const void* f = p.F32 ? reinterpret_cast<const void*>(k_product_f<true, float>)
-                        : reinterpret_cast<const void*>(k_product_f<true, double>);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kProductThreads, product_smem_bytes(p)) != cudaSuccess)
+  const bool st = product_staged(p);
+  const void* f = p.F32 ? (st ? reinterpret_cast<const void*>(k_product_f<true, float, true>)
+                              : reinterpret_cast<const void*>(k_product_f<true, float, false>))
+                        : (st ? reinterpret_cast<const void*>(k_product_f<true, double, true>)
+                              : reinterpret_cast<const void*>(k_product_f<true, double, false>));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, product_threads(p), product_smem_bytes(p)) != cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
 }
@@ -1374,12 +1405,21 @@ void launch_pcg_init(const Params& p, cudaStream_t s) { k_pcg_init<<<1, 1024, 0,
 void launch_product(const Params& p, cudaStream_t s) {
   if (p.factored) {
     const size_t smem = product_smem_bytes(p);
-    if (p.F32) {
-      if (p.shared) k_product_f<true, float><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
-      else k_product_f<false, float><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
+    const int nt = product_threads(p);
+    if (product_staged(p)) {
+      if (p.F32) {
+        if (p.shared) k_product_f<true, float, true><<<p.prod_blocks, nt, smem, s>>>(p);
+        else k_product_f<false, float, true><<<p.prod_blocks, nt, smem, s>>>(p);
+      } else {
+        if (p.shared) k_product_f<true, double, true><<<p.prod_blocks, nt, smem, s>>>(p);
+        else k_product_f<false, double, true><<<p.prod_blocks, nt, smem, s>>>(p);
+      }
+    } else if (p.F32) {
+      if (p.shared) k_product_f<true, float, false><<<p.prod_blocks, nt, smem, s>>>(p);
+      else k_product_f<false, float, false><<<p.prod_blocks, nt, smem, s>>>(p);
     } else {
-      if (p.shared) k_product_f<true, double><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
-      else k_product_f<false, double><<<p.prod_blocks, kProductThreads, smem, s>>>(p);
+      if (p.shared) k_product_f<true, double, false><<<p.prod_blocks, nt, smem, s>>>(p);
+      else k_product_f<false, double, false><<<p.prod_blocks, nt, smem, s>>>(p);
     }
     return;
   }
