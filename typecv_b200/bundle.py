@@ -79,6 +79,12 @@ class ShadeDevice:
 
 # ---- validation (src/geometry/validation.ts:6-46, camera.ts:5-12, pose.ts:18-31) ---------------
 
+def camera_center_of(pose) -> list[float]:
+    """cameraCenter (src/geometry/pose.ts:34-39): -R^T t, in the reference's order of operations."""
+    R, t = pose["R"], pose["t"]
+    return [-float(R[i]) * float(t[0]) - float(R[i + 3]) * float(t[1]) - float(R[i + 6]) * float(t[2]) for i in range(3)]
+
+
 def _safe_int(v) -> bool:
     return isinstance(v, (int, np.integer)) and not isinstance(v, bool) and abs(int(v)) <= 2**53 - 1
 
@@ -329,12 +335,10 @@ def check_bundle_output(values: np.ndarray, base: int) -> None:
 _WG = (32, 64, 128, 256, "auto")
 
 
-def bundle_adjust_gpu(device: ShadeDevice, inp: dict, options: dict | None = None, *,
-                      precision: str = "fp64") -> dict[str, Any]:
-    """Jointly optimise camera poses, points and (with ``refineSharedFocal``) one shared
-    log-focal scale on the GPU (bundleAdjustGpu, src/sfm/bundle/gpu/bundle.ts:803-839).
-
-    ``precision="mixed"`` selects the mixed-precision form (no reference counterpart)."""
+def prepare_bundle(inp: dict, options: dict | None = None, *, precision: str = "fp64") -> dict[str, Any]:
+    """The host half of bundleAdjustGpu before the device plan (bundle.ts:803-839 up to the
+    upload): option checks, bundleProblem, packBundleScene, finiteGpuArray and the control block.
+    Returns the packed problem with what `finish_bundle` needs to read the result."""
     options = dict(options or {})
     if options.get("cameraProductWorkgroupSize") is not None and options["cameraProductWorkgroupSize"] not in _WG:
         raise RangeError("cameraProductWorkgroupSize must be 32, 64, 128, 256 or auto")
@@ -364,7 +368,15 @@ def bundle_adjust_gpu(device: ShadeDevice, inp: dict, options: dict | None = Non
                            iterations=pb["iterations"], max_cg=pb["maxCg"], shared_focal=shared, huber=pb["huber"],
                            tolerance=pb["tolerance"], stall=stall, directional=P - pb["finitePoints"],
                            precision=_lib.TBA_PRECISION_MIXED if precision == "mixed" else _lib.TBA_PRECISION_FP64)
-    values, report = solve_packed(device, control, scene, index)
+    return {"pb": pb, "model": model, "scene": scene, "index": index, "control": control, "shared": shared,
+            "C": C, "P": P, "M": M}
+
+
+def finish_bundle(values: np.ndarray, report: dict, prepared: dict) -> dict[str, Any]:
+    """The host half of bundleAdjustGpu after the device plan (bundle.ts:773-800): checkBundleOutput,
+    bundleOutputPose / bundleOutputLandmarks / bundleOutputReport, separateBundleDirections."""
+    pb, model, shared = prepared["pb"], prepared["model"], prepared["shared"]
+    C, P, M = prepared["C"], prepared["P"], prepared["M"]
     base = 12 * C + 3 * P
     check_bundle_output(values, base)
     # Preserve fixed host constants exactly (bundle.ts:776-784; joint-focal.ts:902-910).
@@ -389,10 +401,21 @@ def bundle_adjust_gpu(device: ShadeDevice, inp: dict, options: dict | None = Non
                         "observations": M, "baseline": float(st[2])},
         "cgIterations": int(st[16]),
         "linearSolverFailures": int(st[17]),
-        "execution": {"backend": "cuda", "report": report, "applicationUploadBytes": report["h2d_bytes"],
-                      "applicationReadbackBytes": report["d2h_bytes"], "cpuStages": []},
+        "execution": {"backend": "cuda", "report": report, "applicationUploadBytes": report.get("h2d_bytes", 0),
+                      "applicationReadbackBytes": report.get("d2h_bytes", 0), "cpuStages": []},
     }
     return separate_bundle_directions(result, pb["finitePoints"])
+
+
+def bundle_adjust_gpu(device: ShadeDevice, inp: dict, options: dict | None = None, *,
+                      precision: str = "fp64") -> dict[str, Any]:
+    """Jointly optimise camera poses, points and (with ``refineSharedFocal``) one shared
+    log-focal scale on the GPU (bundleAdjustGpu, src/sfm/bundle/gpu/bundle.ts:803-839).
+
+    ``precision="mixed"`` selects the mixed-precision form (no reference counterpart)."""
+    prepared = prepare_bundle(inp, options, precision=precision)
+    values, report = solve_packed(device, prepared["control"], prepared["scene"], prepared["index"])
+    return finish_bundle(values, report, prepared)
 
 
 def separate_bundle_directions(result, finite_points):
