@@ -289,6 +289,44 @@ tba_status tba_bundle_vjp(tba_device* device, const tba_vjp_control* control, co
                           double* pixels_bar, size_t pixels_bar_len, double* intrinsics_bar, double* solution,
                           size_t solution_len, tba_vjp_report* report);
 
+/*
+ * Observation evaluation of a fixed scene: the reference's evaluateObservationsGpu
+ * (src/geometry/gpu/observations.ts:34-125), which the mapper runs after a bundle adjustment to
+ * measure and filter its observations (src/sfm/mapper/mapper.ts:837-858).  Every observation is
+ * projected; it is an inlier when the projection is in the camera model's domain and its error is
+ * within max_error_px.  With max_relative_depth_std > 0 every track whose inliers leave its point's
+ * linearised depth uncertainty (pixel_noise_std_px of independent pixel noise, poses and
+ * intrinsics fixed) above that bound in any inlier camera loses all its inliers.
+ *
+ * The arrays are the reference's observation layout (observationLayout,
+ * src/geometry/gpu/observation-layout.ts): cameras 18 doubles per referenced camera (R row-major,
+ * t, fx, fy, cx, cy, k1, k2), points 3 per point (one point per track), pixels 2 per observation,
+ * indices 2 per observation (camera record, point), offsets P + 1 first observations of each
+ * track (only with the depth bound; observations grouped by track).  flags receives M words (1 =
+ * inlier) and, with the depth bound, P more (1 = the track was rejected); summary receives the
+ * inliers' error sum and their count.
+ */
+typedef struct {
+  uint32_t cameras, points, observations;
+  uint32_t reserved;               /* 0 */
+  double max_error_px;             /* 1e-12..1e6 */
+  double max_relative_depth_std;   /* 0: no depth filter */
+  double pixel_noise_std_px;       /* > 0 (the reference's default is 1) */
+} tba_observation_control;
+
+typedef struct {
+  double upload_ms, evaluate_ms, download_ms, wall_ms;
+  uint64_t h2d_bytes, d2h_bytes;
+  uint32_t kernel_launches;
+} tba_observation_report;
+
+tba_status tba_evaluate_observations(tba_device* device, const tba_observation_control* control,
+                                     const double* cameras, size_t cameras_len, const double* points,
+                                     size_t points_len, const double* pixels, size_t pixels_len,
+                                     const uint32_t* indices, size_t indices_len, const uint32_t* offsets,
+                                     size_t offsets_len, uint32_t* flags, size_t flags_len, double* summary,
+                                     tba_observation_report* report);
+
 #ifdef __cplusplus
 }
 #endif

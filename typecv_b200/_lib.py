@@ -18,7 +18,8 @@ TBA_FLAG_TIME_PRODUCTS = 1
 # Every symbol include/tba.h declares.
 EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
            "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc", "tba_batch_max_cameras",
-           "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust", "tba_bundle_vjp")
+           "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust", "tba_bundle_vjp",
+           "tba_evaluate_observations")
 
 
 class LibraryError(RuntimeError):
@@ -102,6 +103,25 @@ class VjpReport(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ObservationControl(ctypes.Structure):
+    _fields_ = [
+        ("cameras", ctypes.c_uint32), ("points", ctypes.c_uint32), ("observations", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32), ("max_error_px", ctypes.c_double),
+        ("max_relative_depth_std", ctypes.c_double), ("pixel_noise_std_px", ctypes.c_double),
+    ]
+
+
+class ObservationReport(ctypes.Structure):
+    _fields_ = [
+        ("upload_ms", ctypes.c_double), ("evaluate_ms", ctypes.c_double), ("download_ms", ctypes.c_double),
+        ("wall_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -149,6 +169,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                    ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_double),
                                    ctypes.c_size_t, P(ctypes.c_double), P(ctypes.c_double), ctypes.c_size_t,
                                    P(VjpReport)]
+    lib.tba_evaluate_observations.restype = ctypes.c_int
+    lib.tba_evaluate_observations.argtypes = [vp, P(ObservationControl), P(ctypes.c_double), ctypes.c_size_t,
+                                              P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t,
+                                              P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_uint32), ctypes.c_size_t,
+                                              P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_double),
+                                              P(ObservationReport)]
     _lib = lib
     return lib
 

@@ -24,6 +24,7 @@
 #include "tba_adjoint.cuh"
 #include "tba_batch.cuh"
 #include "tba_engine.cuh"
+#include "tba_observations.cuh"
 
 using tba::Params;
 
@@ -1050,6 +1051,87 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   }
 }
 
+// ---- observation evaluation ------------------------------------------------------------------------
+
+void evaluate_observations(tba_device* d, const tba_observation_control* oc, const double* cameras,
+                           const double* points, const double* pixels, const uint32_t* indices,
+                           const uint32_t* offsets, uint32_t* flags, double* summary, tba_observation_report* report) {
+  const auto wall0 = std::chrono::steady_clock::now();
+  const uint32_t C = oc->cameras, P = oc->points, M = oc->observations;
+  const bool guarded = oc->max_relative_depth_std > 0;
+  Layout L;
+  const size_t o_cam = L.take<double>(18 * size_t(C)), o_pts = L.take<double>(3 * size_t(P)),
+               o_pix = L.take<double>(2 * size_t(M)), o_idx = L.take<uint32_t>(2 * size_t(M)),
+               o_off = L.take<uint32_t>(guarded ? size_t(P) + 1 : 0),
+               o_flags = L.take<uint32_t>(size_t(M) + (guarded ? P : 0)), o_err = L.take<double>(M),
+               o_part = L.take<double>(2 * ((size_t(M) + 63) / 64)), o_sum = L.take<double>(2);
+  if (d->capacity < L.bytes) {
+    if (d->arena) CUDA_TRY(cudaFree(d->arena));
+    d->arena = nullptr;
+    d->capacity = 0;
+    size_t free_bytes = 0, total_bytes = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_bytes, &total_bytes));
+    if (L.bytes > free_bytes)
+      throw Fail{TBA_ERROR_BUDGET, "GPU observation evaluation exceeds budget"};
+    CUDA_TRY(cudaMalloc(&d->arena, L.bytes));
+    d->capacity = L.bytes;
+  }
+  char* a = d->arena;
+  tba::ObsParams p{};
+  p.C = C;
+  p.P = P;
+  p.M = M;
+  p.guarded = guarded ? 1 : 0;
+  p.max_error = oc->max_error_px;
+  p.max_relative_depth = oc->max_relative_depth_std;
+  p.noise = oc->pixel_noise_std_px;
+  p.cameras = reinterpret_cast<double*>(a + o_cam);
+  p.points = reinterpret_cast<double*>(a + o_pts);
+  p.pixels = reinterpret_cast<double*>(a + o_pix);
+  p.indices = reinterpret_cast<uint32_t*>(a + o_idx);
+  p.offsets = guarded ? reinterpret_cast<uint32_t*>(a + o_off) : nullptr;
+  p.flags = reinterpret_cast<uint32_t*>(a + o_flags);
+  p.errors = reinterpret_cast<double*>(a + o_err);
+  p.partials = reinterpret_cast<double*>(a + o_part);
+  p.summary = reinterpret_cast<double*>(a + o_sum);
+  cudaStream_t s = d->stream;
+  cudaEvent_t e0 = event(d, 0), e1 = event(d, 1), e2 = event(d, 2), e3 = event(d, 3);
+  uint64_t h2d = 0;
+  auto up = [&](size_t off, const void* src, size_t bytes) {
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(a + off, src, bytes, cudaMemcpyHostToDevice, s));
+    h2d += bytes;
+  };
+  CUDA_TRY(cudaEventRecord(e0, s));
+  up(o_cam, cameras, 18 * sizeof(double) * C);
+  up(o_pts, points, 3 * sizeof(double) * P);
+  up(o_pix, pixels, 2 * sizeof(double) * M);
+  up(o_idx, indices, 2 * sizeof(uint32_t) * M);
+  if (guarded) up(o_off, offsets, sizeof(uint32_t) * (size_t(P) + 1));
+  CUDA_TRY(cudaEventRecord(e1, s));
+  tba::launch_observations(p, s);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaEventRecord(e2, s));
+  const size_t nflags = size_t(M) + (guarded ? P : 0);
+  if (nflags) CUDA_TRY(cudaMemcpyAsync(flags, p.flags, nflags * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(summary, p.summary, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaEventRecord(e3, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (report) {
+    std::memset(report, 0, sizeof *report);
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    report->upload_ms = ms;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e1, e2));
+    report->evaluate_ms = ms;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e2, e3));
+    report->download_ms = ms;
+    report->h2d_bytes = h2d;
+    report->d2h_bytes = nflags * sizeof(uint32_t) + 2 * sizeof(double);
+    report->kernel_launches = (M ? 1u : 0u) + (guarded && P ? 1u : 0u) + (M ? 1u : 0u) + 1u;
+    report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1218,6 +1300,66 @@ tba_status tba_bundle_vjp(tba_device* d, const tba_vjp_control* vc, const double
     check_scene(&c, scene, scene_len);
     CUDA_TRY(cudaSetDevice(d->ordinal));
     solve_vjp(d, vc, scene, index, cotangent, pixels_bar, intrinsics_bar, solution, report);
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
+  } catch (const std::exception& e) {
+    d->error = e.what();
+    return TBA_ERROR_INTERNAL;
+  }
+  return TBA_OK;
+}
+
+tba_status tba_evaluate_observations(tba_device* d, const tba_observation_control* oc, const double* cameras,
+                                     size_t cameras_len, const double* points, size_t points_len, const double* pixels,
+                                     size_t pixels_len, const uint32_t* indices, size_t indices_len,
+                                     const uint32_t* offsets, size_t offsets_len, uint32_t* flags, size_t flags_len,
+                                     double* summary, tba_observation_report* report) {
+  if (!d) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (!oc || !summary) argument("Invalid GPU observation request");
+    const uint64_t C = oc->cameras, P = oc->points, M = oc->observations;
+    const bool guarded = oc->max_relative_depth_std > 0;
+    if (!(std::isfinite(oc->max_error_px) && oc->max_error_px >= 1e-12 && oc->max_error_px <= 1e6) ||
+        !(std::isfinite(oc->max_relative_depth_std) && oc->max_relative_depth_std >= 0 &&
+          oc->max_relative_depth_std <= 1e9) ||
+        !(std::isfinite(oc->pixel_noise_std_px) && oc->pixel_noise_std_px > 0 && oc->pixel_noise_std_px <= 1e9))
+      argument("Invalid GPU observation threshold");
+    if (2 * M + P + 1 > 0xffffffffull || 18 * C > 0xffffffffull) argument("GPU observation evaluation exceeds budget");
+    if ((C && !cameras) || (P && !points) || (M && (!pixels || !indices)) || ((M || guarded) && !flags))
+      argument("Invalid GPU observation arrays: null pointer");
+    if (cameras_len < 18 * C || points_len < 3 * P || pixels_len < 2 * M || indices_len < 2 * M ||
+        flags_len < M + (guarded ? P : 0))
+      argument("Invalid GPU observation arrays: lengths");
+    FirstFailure ff;
+    parallel_ranges(M, 1u << 18, [&](uint64_t b, uint64_t e, unsigned) {
+      for (uint64_t i = b; i < e; i++)
+        if (indices[2 * i] >= C || indices[2 * i + 1] >= P)
+          return ff.record(i, "Invalid GPU observation indices: a camera or point out of range");
+    });
+    ff.raise();
+    if (guarded) {
+      if (!offsets || offsets_len < P + 1) argument("Invalid GPU observation arrays: track offsets");
+      if (offsets[0] != 0 || offsets[P] != M) argument("Invalid GPU observation arrays: track offsets");
+      for (uint64_t h = 0; h < P; h++) {
+        if (offsets[h + 1] < offsets[h]) argument("Invalid GPU observation arrays: track offsets");
+        for (uint64_t i = offsets[h]; i < offsets[h + 1]; i++)
+          if (indices[2 * i + 1] != h) argument("Invalid GPU observation arrays: track offsets");
+      }
+    }
+    auto bounded = [](const double* v, uint64_t n) {
+      for (uint64_t i = 0; i < n; i++) {
+        const double x = v[i];
+        if (!std::isfinite(x) || std::fabs(x) > 1e9 || (x != 0 && std::fabs(x) < 1e-30)) return false;
+      }
+      return true;
+    };
+    if (!bounded(cameras, 18 * C) || !bounded(points, 3 * P) || !bounded(pixels, 2 * M))
+      argument("Invalid GPU scene coordinate bounds");
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    evaluate_observations(d, oc, cameras, points, pixels, indices, offsets, flags, summary, report);
   } catch (const Fail& f) {
     d->error = f.message;
     return f.status;

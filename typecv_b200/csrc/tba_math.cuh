@@ -101,6 +101,26 @@ __host__ __device__ inline bool inverse3_spd(const double a[9], double out[6]) {
   return true;
 }
 
+// solve3: x = a^-1 b by the equilibrated Cholesky factorisation of the SPD block `a` (row-major),
+// with the same pivot floors as inverse3_spd; false when `a` is not safely positive definite.
+__host__ __device__ inline bool solve3_spd(const double a[9], const double b[3], double x[3]) {
+  if (!(fmin(a[0], fmin(a[4], a[8])) > 0)) return false;
+  const double d0 = 1 / sqrt(a[0]), d1 = 1 / sqrt(a[4]), d2 = 1 / sqrt(a[8]);
+  const double l10 = a[3] * d0 * d1, l20 = a[6] * d0 * d2;
+  const double pivot1 = 1 - l10 * l10;
+  if (!(pivot1 > 1e-14)) return false;
+  const double l11 = sqrt(pivot1), l21 = (a[7] * d1 * d2 - l20 * l10) / l11;
+  const double pivot2 = 1 - l20 * l20 - l21 * l21;
+  if (!(pivot2 > 1e-14)) return false;
+  const double l22 = sqrt(pivot2), y0 = b[0] * d0;
+  const double y1 = (b[1] * d1 - l10 * y0) / l11, y2 = (b[2] * d2 - l20 * y0 - l21 * y1) / l22;
+  const double x2 = y2 / l22, x1 = (y1 - l21 * x2) / l11, x0 = y0 - l10 * x1 - l20 * x2;
+  x[0] = x0 * d0;
+  x[1] = x1 * d1;
+  x[2] = x2 * d2;
+  return true;
+}
+
 // Index of entry (i, j) of a symmetric 6x6 block stored as its lower triangle, row by row.
 __host__ __device__ constexpr int sym6(int i, int j) {
   return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;

@@ -1,0 +1,163 @@
+// Observation evaluation of a fixed scene (evaluateObservationsGpu,
+// src/geometry/gpu/observations.ts:34-125; kernels of src/geometry/gpu/observation-evaluation.shade.ts),
+// sm_100a, FP64.
+//
+//   k_obs_project   per observation: project the point in its camera; an inlier when the
+//                   projection is in the model's domain and its error is within the threshold
+//                   (projectIndexedObservations)
+//   k_obs_depth     per track (only with a depth bound): the linearised depth sensitivity of the
+//                   track's point to independent pixel noise, from its inlier observations with the
+//                   poses and intrinsics fixed; a track above the bound loses all its inliers
+//                   (filterIndexedObservationDepth, stableDepth)
+//   k_obs_partials  the inlier error sum and count of each run of 64 observations, each run summed
+//                   in order (indexedObservationPartials), then k_obs_summary sums the runs in a
+//                   fixed tree (observationSummary)
+//
+// Layout (observationLayout, src/geometry/gpu/observation-layout.ts): one 18-word record per
+// referenced camera (pose R row-major, t, then fx, fy, cx, cy, k1, k2), 3 words per point, 2 per
+// observation pixel, and per observation its camera and point index interleaved.
+#include <cuda_runtime.h>
+
+#include "tba_math.cuh"
+#include "tba_observations.cuh"
+
+namespace tba {
+namespace {
+
+__device__ inline void obs_camera(const ObsParams& A, uint32_t i, double pose[12], Camera& k) {
+  const double* r = A.cameras + 18 * size_t(A.indices[2 * size_t(i)]);
+  for (int j = 0; j < 12; j++) pose[j] = r[j];
+  k = Camera{r[12], r[13], r[14], r[15], r[16], r[17]};
+}
+
+__device__ inline void obs_transform(const double pose[12], const double* X, double q[3]) {
+  for (int r = 0; r < 3; r++) q[r] = pose[3 * r] * X[0] + pose[3 * r + 1] * X[1] + pose[3 * r + 2] * X[2] + pose[9 + r];
+}
+
+__global__ void __launch_bounds__(256) k_obs_project(ObsParams A) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.M) return;
+  A.flags[i] = 0;
+  A.errors[i] = 0;
+  double pose[12], q[3], pixel[2], du[3], dv[3];
+  Camera k;
+  obs_camera(A, i, pose, k);
+  obs_transform(pose, A.points + 3 * size_t(A.indices[2 * size_t(i) + 1]), q);
+  if (!project(k, q, pixel, du, dv)) return;
+  const double x = pixel[0] - A.pixels[2 * size_t(i)], y = pixel[1] - A.pixels[2 * size_t(i) + 1];
+  const double e = sqrt(x * x + y * y);
+  if (e <= A.max_error) {
+    A.flags[i] = 1;
+    A.errors[i] = e;
+  }
+}
+
+// stableDepth: the information matrix of the point from the inlier observations (unweighted point
+// Jacobians), then for each inlier the variance of its camera-frame depth, sigma_z^2 = a^T A^-1 a
+// with a the camera's optical axis, against the relative bound noise * sigma_z / z.
+__device__ bool obs_stable_depth(const ObsParams& A, uint32_t start, uint32_t end, const double* X) {
+  double M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t count = 0;
+  for (uint32_t i = start; i < end; i++) {
+    if (A.flags[i] == 0) continue;
+    count++;
+    double pose[12], q[3], pixel[2], du[3], dv[3];
+    Camera k;
+    obs_camera(A, i, pose, k);
+    obs_transform(pose, X, q);
+    if (!project(k, q, pixel, du, dv)) return false;
+    for (int row = 0; row < 2; row++) {
+      const double* g = row == 0 ? du : dv;
+      const double J[3] = {g[0] * pose[0] + g[1] * pose[3] + g[2] * pose[6],
+                           g[0] * pose[1] + g[1] * pose[4] + g[2] * pose[7],
+                           g[0] * pose[2] + g[1] * pose[5] + g[2] * pose[8]};
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) M[3 * r + c] += J[r] * J[c];
+    }
+  }
+  if (count < 2) return false;
+  for (uint32_t i = start; i < end; i++) {
+    if (A.flags[i] == 0) continue;
+    double pose[12], q[3], s[3];
+    Camera k;
+    obs_camera(A, i, pose, k);
+    const double axis[3] = {pose[6], pose[7], pose[8]};
+    obs_transform(pose, X, q);
+    if (!solve3_spd(M, axis, s) || !(q[2] > 0)) return false;
+    const double variance = axis[0] * s[0] + axis[1] * s[1] + axis[2] * s[2];
+    if (!(variance >= 0)) return false;
+    const double relative = A.noise * sqrt(variance) / q[2];
+    if (!(relative <= A.max_relative_depth)) return false;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_obs_depth(ObsParams A) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= A.P) return;
+  const uint32_t start = A.offsets[h], end = A.offsets[h + 1];
+  A.flags[A.M + h] = 0;
+  if (end <= start) return;
+  uint32_t accepted = 0;
+  for (uint32_t i = start; i < end; i++) accepted += A.flags[i] != 0;
+  if (accepted < 2) return;
+  if (!obs_stable_depth(A, start, end, A.points + 3 * size_t(A.indices[2 * size_t(start) + 1]))) {
+    A.flags[A.M + h] = 1;
+    for (uint32_t i = start; i < end; i++) {
+      A.flags[i] = 0;
+      A.errors[i] = 0;
+    }
+  }
+}
+
+// One thread per run of 64 observations: its inlier error sum (in order) and inlier count.
+__global__ void __launch_bounds__(256) k_obs_partials(ObsParams A) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t runs = (A.M + 63) / 64;
+  if (b >= runs) return;
+  double e = 0, n = 0;
+  const uint32_t end = min(A.M, 64 * b + 64);
+  for (uint32_t i = 64 * b; i < end; i++)
+    if (A.flags[i] != 0) {
+      e += A.errors[i];
+      n += 1;
+    }
+  A.partials[2 * size_t(b)] = e;
+  A.partials[2 * size_t(b) + 1] = n;
+}
+
+__global__ void __launch_bounds__(1024) k_obs_summary(ObsParams A) {
+  __shared__ double se[1024], sn[1024];
+  const uint32_t runs = (A.M + 63) / 64;
+  double e = 0, n = 0;
+  for (uint32_t b = threadIdx.x; b < runs; b += blockDim.x) {
+    e += A.partials[2 * size_t(b)];
+    n += A.partials[2 * size_t(b) + 1];
+  }
+  se[threadIdx.x] = e;
+  sn[threadIdx.x] = n;
+  __syncthreads();
+  for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      se[threadIdx.x] += se[threadIdx.x + s];
+      sn[threadIdx.x] += sn[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    A.summary[0] = se[0];
+    A.summary[1] = sn[0];
+  }
+}
+
+}  // namespace
+
+void launch_observations(const ObsParams& a, cudaStream_t s) {
+  if (a.M) k_obs_project<<<(a.M + 255) / 256, 256, 0, s>>>(a);
+  if (a.guarded && a.P) k_obs_depth<<<(a.P + 127) / 128, 128, 0, s>>>(a);
+  const uint32_t runs = (a.M + 63) / 64;
+  if (runs) k_obs_partials<<<(runs + 255) / 256, 256, 0, s>>>(a);
+  k_obs_summary<<<1, 1024, 0, s>>>(a);
+}
+
+}  // namespace tba

@@ -1,0 +1,27 @@
+// Observation evaluation of a fixed scene (tba_observations.cu): device parameters and launch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace tba {
+
+struct ObsParams {
+  uint32_t C, P, M;  // camera records, points (= tracks), observations
+  uint32_t guarded;  // 1: the depth-sensitivity filter runs (offsets are given)
+  double max_error, max_relative_depth, noise;
+  const double* cameras;   // 18 per camera record
+  const double* points;    // 3P
+  const double* pixels;    // 2M
+  const uint32_t* indices;  // 2M: camera record, point
+  const uint32_t* offsets;  // P + 1 first observations of each track (guarded)
+  uint32_t* flags;          // M (+ P with the depth filter: 1 = the track was rejected)
+  double* errors;           // M
+  double* partials;         // 2 per run of 64 observations
+  double* summary;          // inlier error sum, inlier count
+};
+
+void launch_observations(const ObsParams& a, cudaStream_t s);
+
+}  // namespace tba
