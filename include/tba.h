@@ -135,6 +135,30 @@ tba_status tba_bundle_adjust(tba_device* device, const tba_control* control, con
                              double* output, size_t output_len, tba_report* report);
 
 /*
+ * A resident scene: the packed arrays of one problem kept on the device between adjustments, so
+ * that repeated adjustments of the same map (the mapper's refinement passes) neither re-check nor
+ * re-upload them.  It replaces the reference's per-call packing and upload
+ * (packBundleScene, src/sfm/bundle/gpu/bundle-host.ts:177-218; bundle.ts:267-271) for callers that
+ * keep the map in the packed layout (the reference's HostScene strides, src/sfm/scene/scene.ts:8-131).
+ *
+ * tba_scene_create checks and uploads the arrays once (as tba_bundle_adjust does per call);
+ * tba_scene_adjust runs a bundle adjustment on them and leaves the solution's poses and points in
+ * the scene, so the next adjustment starts from it.  `control` must have the scene's sizes and
+ * gauge; its solver options may change between calls.  output (the tba_bundle_adjust record) and
+ * state (its 26 [+1] state words) are optional.  tba_scene_write replaces the poses and/or points
+ * (NULL: keep), tba_scene_read copies them out.  A scene belongs to the device handle it was created
+ * on and is released by tba_scene_destroy.
+ */
+typedef struct tba_scene tba_scene;
+tba_status tba_scene_create(tba_device* device, const tba_control* shape, const double* scene, size_t scene_len,
+                            const uint32_t* index, size_t index_len, tba_scene** out);
+void tba_scene_destroy(tba_scene* scene);
+tba_status tba_scene_adjust(tba_device* device, tba_scene* scene, const tba_control* control, double* output,
+                            size_t output_len, double* state, size_t state_len, tba_report* report);
+tba_status tba_scene_write(tba_device* device, tba_scene* scene, const double* poses, const double* points);
+tba_status tba_scene_read(tba_device* device, tba_scene* scene, double* poses, double* points);
+
+/*
  * The robust cost of a packed scene that is already in device memory, computed without
  * allocating.  No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc — applications whose device memory belongs to their own allocator (a caching pool

@@ -19,7 +19,8 @@ TBA_FLAG_TIME_PRODUCTS = 1
 EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
            "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc", "tba_batch_max_cameras",
            "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust", "tba_bundle_vjp",
-           "tba_evaluate_observations")
+           "tba_evaluate_observations", "tba_scene_create", "tba_scene_destroy", "tba_scene_adjust",
+           "tba_scene_write", "tba_scene_read")
 
 
 class LibraryError(RuntimeError):
@@ -175,6 +176,18 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                               P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_uint32), ctypes.c_size_t,
                                               P(ctypes.c_uint32), ctypes.c_size_t, P(ctypes.c_double),
                                               P(ObservationReport)]
+    lib.tba_scene_create.restype = ctypes.c_int
+    lib.tba_scene_create.argtypes = [vp, P(Control), P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_uint32),
+                                     ctypes.c_size_t, P(vp)]
+    lib.tba_scene_destroy.restype = None
+    lib.tba_scene_destroy.argtypes = [vp]
+    lib.tba_scene_adjust.restype = ctypes.c_int
+    lib.tba_scene_adjust.argtypes = [vp, vp, P(Control), P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_double),
+                                     ctypes.c_size_t, P(Report)]
+    lib.tba_scene_write.restype = ctypes.c_int
+    lib.tba_scene_write.argtypes = [vp, vp, P(ctypes.c_double), P(ctypes.c_double)]
+    lib.tba_scene_read.restype = ctypes.c_int
+    lib.tba_scene_read.argtypes = [vp, vp, P(ctypes.c_double), P(ctypes.c_double)]
     _lib = lib
     return lib
 

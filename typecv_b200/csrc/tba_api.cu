@@ -47,6 +47,16 @@ struct tba_device {
   std::map<std::string, int> tuned;
 };
 
+// A scene resident on the device between calls: the packed arrays of one problem and its host
+// schedules.
+struct tba_scene {
+  tba_device* device = nullptr;
+  tba_control shape{};
+  double* scene = nullptr;     // device, tba_scene_size doubles
+  uint32_t* index = nullptr;   // device, tba_index_size words
+  void* plan = nullptr;        // HostPlan
+};
+
 namespace {
 
 std::string g_open_error;
@@ -263,20 +273,52 @@ cudaEvent_t event(tba_device* d, size_t k) {
   return d->events[k];
 }
 
+// The host-side schedules of one problem's index: warp tasks (with their first observations),
+// camera chunks and the number of fixed cameras.
+struct HostPlan {
+  std::vector<uint32_t> tasks, task_obs;
+  Chunks chunks;
+  uint32_t fixed = 0;
+};
+
+HostPlan make_plan(const tba_control* ctl, const uint32_t* index, int sms) {
+  const uint32_t C = ctl->cameras, P = ctl->points, M = ctl->observations;
+  const uint32_t* ps = index + 2 * size_t(M);
+  const uint32_t* cs = ps + P + 1;
+  const uint32_t* active = cs + C + 1 + M;
+  HostPlan plan;
+  plan.tasks = build_tasks(ps, P);
+  plan.task_obs.resize(plan.tasks.size());
+  for (size_t t = 0; t < plan.tasks.size(); t++) plan.task_obs[t] = ps[plan.tasks[t]];
+  plan.chunks = build_chunks(cs, C, M, sms);
+  for (uint32_t c = 0; c < C; c++) plan.fixed += active[c] == 0;
+  return plan;
+}
+
+// Where a solve reads its problem and where it leaves the solution.  With `device_source` the
+// scene and index are device pointers (a resident scene) and `plan` is given; `writeback` (device)
+// receives the solved poses and points; `output` may be null and `state` (host) receives the
+// result's state words.
+struct SolveIO {
+  bool device_source = false;
+  const HostPlan* plan = nullptr;
+  double* writeback = nullptr;
+  double* state = nullptr;
+};
+
 void solve(tba_device* d, const tba_control* ctl, const double* scene, const uint32_t* index,
-           double* output, tba_report* report) {
+           double* output, tba_report* report, const SolveIO& io = SolveIO()) {
   const auto wall0 = std::chrono::steady_clock::now();
   const uint32_t C = ctl->cameras, P = ctl->points, M = ctl->observations;
   const bool shared = ctl->shared_focal != 0;
   const uint32_t m = 6 * C + (shared ? 1 : 0);
-  const uint32_t* ps = index + 2 * size_t(M);
-  const uint32_t* cs = ps + P + 1;
-  const uint32_t* active = cs + C + 1 + M;
-  const std::vector<uint32_t> tasks = build_tasks(ps, P);
-  const Chunks chunks = build_chunks(cs, C, M, d->sms);
+  HostPlan own;
+  if (!io.plan) own = make_plan(ctl, index, d->sms);
+  const HostPlan& plan = io.plan ? *io.plan : own;
+  const std::vector<uint32_t>& tasks = plan.tasks;
+  const Chunks& chunks = plan.chunks;
   const uint32_t ntasks = uint32_t(tasks.size() - 1), nchunks = uint32_t(chunks.cam.size());
-  uint32_t fixed = 0;
-  for (uint32_t c = 0; c < C; c++) fixed += active[c] == 0;
+  const uint32_t fixed = plan.fixed;
 
   Params p{};
   p.C = C;
@@ -395,7 +437,12 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   size_t ev = 0;
   cudaEvent_t e_start = event(d, ev++), e_up = event(d, ev++), e_solved = event(d, ev++), e_down = event(d, ev++);
   uint64_t h2d = 0;
+  // Problem arrays: host-to-device, or device-to-device from a resident scene.
   auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, io.device_source ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    if (!io.device_source) h2d += bytes;
+  };
+  auto up_host = [&](void* dst, const void* src, size_t bytes) {
     if (bytes) CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
     h2d += bytes;
   };
@@ -405,13 +452,11 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   up(const_cast<double*>(p.cams), scene + 12 * size_t(C) + 3 * size_t(P), 6 * sizeof(double) * C);
   up(const_cast<double*>(p.pixels), scene + 18 * size_t(C) + 3 * size_t(P), 2 * sizeof(double) * M);
   up(dindex, index, sizeof(uint32_t) * (3 * size_t(M) + P + 2 * size_t(C) + 2));
-  up(U32(o_tasks), tasks.data(), sizeof(uint32_t) * tasks.size());
-  std::vector<uint32_t> task_obs(tasks.size());
-  for (size_t t = 0; t < tasks.size(); t++) task_obs[t] = ps[tasks[t]];
-  up(U32(o_tobs), task_obs.data(), sizeof(uint32_t) * task_obs.size());
-  up(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
-  up(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
-  up(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
+  up_host(U32(o_tasks), tasks.data(), sizeof(uint32_t) * tasks.size());
+  up_host(U32(o_tobs), plan.task_obs.data(), sizeof(uint32_t) * plan.task_obs.size());
+  up_host(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
+  up_host(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
+  up_host(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
   CUDA_TRY(cudaEventRecord(e_up, s));
 
   uint32_t launches = 0, lm_done = 0, refinements = 0;
@@ -499,7 +544,21 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaEventRecord(e_solved, s));
   const size_t out_len = 12 * size_t(C) + 3 * size_t(P) + 26 + (shared ? 1 : 0);
-  CUDA_TRY(cudaMemcpyAsync(output, p.output, out_len * sizeof(double), cudaMemcpyDeviceToHost, s));
+  const size_t state_len = 26 + (shared ? 1 : 0);
+  size_t d2h = 0;
+  if (output) {
+    CUDA_TRY(cudaMemcpyAsync(output, p.output, out_len * sizeof(double), cudaMemcpyDeviceToHost, s));
+    d2h += out_len * sizeof(double);
+  }
+  if (io.state) {
+    CUDA_TRY(cudaMemcpyAsync(io.state, p.output + 12 * size_t(C) + 3 * size_t(P), state_len * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    d2h += state_len * sizeof(double);
+  }
+  if (io.writeback) {
+    CUDA_TRY(cudaMemcpyAsync(io.writeback, p.poses, 12 * sizeof(double) * C, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(io.writeback + 12 * size_t(C), p.points, 3 * sizeof(double) * P, cudaMemcpyDeviceToDevice, s));
+  }
   CUDA_TRY(cudaEventRecord(e_down, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   if (report) {
@@ -525,10 +584,11 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     report->product_ms = total;
     report->product_launches = counted;
     report->h2d_bytes = h2d;
-    report->d2h_bytes = out_len * sizeof(double);
+    report->d2h_bytes = d2h;
     report->kernel_launches = launches;
     report->lm_iterations = lm_done;
-    report->cg_iterations = uint32_t(output[12 * size_t(C) + 3 * size_t(P) + tba::S_CG_STEPS]);
+    const double* st = output ? output + 12 * size_t(C) + 3 * size_t(P) : io.state;
+    report->cg_iterations = st ? uint32_t(st[tba::S_CG_STEPS]) : 0;
     report->engine = p.factored ? 0 : 1;
     report->product_blocks = p.factored ? p.prod_blocks : 0;
     report->refinements = uint32_t(refinements);
@@ -1366,6 +1426,139 @@ tba_status tba_evaluate_observations(tba_device* d, const tba_observation_contro
   } catch (const std::exception& e) {
     d->error = e.what();
     return TBA_ERROR_INTERNAL;
+  }
+  return TBA_OK;
+}
+
+tba_status tba_scene_create(tba_device* d, const tba_control* shape, const double* scene, size_t scene_len,
+                            const uint32_t* index, size_t index_len, tba_scene** out) {
+  if (!d || !out) return TBA_ERROR_ARGUMENT;
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  tba_scene* r = nullptr;
+  try {
+    check_control(shape);
+    if (!scene || !index) argument("Invalid GPU BA arrays: null pointer");
+    if (scene_len != tba_scene_size(shape)) argument("Invalid GPU BA scene array length");
+    if (index_len != tba_index_size(shape)) argument("Invalid GPU BA index array length");
+    if (uint64_t(3) * shape->observations + shape->points + 2ull * shape->cameras + 2 > 0xffffffffull)
+      argument("GPU BA scene dimensions exceed integer index bounds");
+    check_index(shape, index);
+    check_scene(shape, scene, scene_len);
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    r = new tba_scene();
+    r->device = d;
+    r->shape = *shape;
+    r->plan = new HostPlan(make_plan(shape, index, d->sms));
+    CUDA_TRY(cudaMalloc(&r->scene, scene_len * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&r->index, index_len * sizeof(uint32_t)));
+    CUDA_TRY(cudaMemcpyAsync(r->scene, scene, scene_len * sizeof(double), cudaMemcpyHostToDevice, d->stream));
+    CUDA_TRY(cudaMemcpyAsync(r->index, index, index_len * sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  } catch (const Fail& f) {
+    d->error = f.message;
+    if (r) {
+      if (r->scene) cudaFree(r->scene);
+      if (r->index) cudaFree(r->index);
+      delete static_cast<HostPlan*>(r->plan);
+      delete r;
+    }
+    return f.status;
+  }
+  *out = r;
+  return TBA_OK;
+}
+
+void tba_scene_destroy(tba_scene* r) {
+  if (!r) return;
+  {
+    std::lock_guard<std::mutex> lock(r->device->mu);
+    cudaSetDevice(r->device->ordinal);
+    cudaStreamSynchronize(r->device->stream);
+    if (r->scene) cudaFree(r->scene);
+    if (r->index) cudaFree(r->index);
+  }
+  delete static_cast<HostPlan*>(r->plan);
+  delete r;
+}
+
+tba_status tba_scene_adjust(tba_device* d, tba_scene* r, const tba_control* control, double* output,
+                            size_t output_len, double* state, size_t state_len, tba_report* report) {
+  if (!d || !r) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (r->device != d) argument("Invalid GPU BA resident scene: it belongs to another device handle");
+    check_control(control);
+    const tba_control& s = r->shape;
+    if (control->cameras != s.cameras || control->points != s.points || control->observations != s.observations ||
+        control->directional_points != s.directional_points || control->anchor != s.anchor ||
+        control->scale_view != s.scale_view)
+      argument("Invalid GPU BA resident scene: the control's sizes or gauge differ from the scene's");
+    if (output && output_len < tba_output_size(control)) argument("Invalid GPU BA output array length");
+    if (state && state_len < size_t(26 + (control->shared_focal ? 1 : 0))) argument("Invalid GPU BA state array length");
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    SolveIO io;
+    io.device_source = true;
+    io.plan = static_cast<const HostPlan*>(r->plan);
+    io.writeback = r->scene;
+    io.state = state;
+    solve(d, control, r->scene, r->index, output, report, io);
+    if (report) report->check_ms = 0;
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
+  } catch (const std::exception& e) {
+    d->error = e.what();
+    return TBA_ERROR_INTERNAL;
+  }
+  return TBA_OK;
+}
+
+tba_status tba_scene_write(tba_device* d, tba_scene* r, const double* poses, const double* points) {
+  if (!d || !r) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (r->device != d) argument("Invalid GPU BA resident scene: it belongs to another device handle");
+    const size_t C = r->shape.cameras, P = r->shape.points;
+    auto bounded = [](const double* v, size_t n) {
+      for (size_t i = 0; i < n; i++) {
+        const double x = v[i];
+        if (!std::isfinite(x) || std::fabs(x) > 1e9 || (x != 0 && std::fabs(x) < 1e-30)) return false;
+      }
+      return true;
+    };
+    if ((poses && !bounded(poses, 12 * C)) || (points && !bounded(points, 3 * P)))
+      argument("GPU BA input exceeds supported coordinate bounds");
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    if (poses) CUDA_TRY(cudaMemcpyAsync(r->scene, poses, 12 * C * sizeof(double), cudaMemcpyHostToDevice, d->stream));
+    if (points)
+      CUDA_TRY(cudaMemcpyAsync(r->scene + 12 * C, points, 3 * P * sizeof(double), cudaMemcpyHostToDevice, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
+  }
+  return TBA_OK;
+}
+
+tba_status tba_scene_read(tba_device* d, tba_scene* r, double* poses, double* points) {
+  if (!d || !r) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (r->device != d) argument("Invalid GPU BA resident scene: it belongs to another device handle");
+    const size_t C = r->shape.cameras, P = r->shape.points;
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    if (poses) CUDA_TRY(cudaMemcpyAsync(poses, r->scene, 12 * C * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+    if (points)
+      CUDA_TRY(cudaMemcpyAsync(points, r->scene + 12 * C, 3 * P * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
   }
   return TBA_OK;
 }
