@@ -351,6 +351,20 @@ tba_status tba_evaluate_observations(tba_device* device, const tba_observation_c
                                      size_t offsets_len, uint32_t* flags, size_t flags_len, double* summary,
                                      tba_observation_report* report);
 
+/*
+ * The measurement linearisation of the inverse-depth bundle adjustment: the device half of the
+ * reference's linearizeInverseDepthGpu / bundleAdjustInverseDepthGpu
+ * (src/sfm/depth/gpu/inverse-depth.ts:15-141, kernel inverse-depth.shade.ts), whose reduced solve
+ * stays on the host in FP64.  measurements: 34 doubles per observation (a, b, rho of the anchored
+ * point; the reference pose; the observing pose; the observing camera record; its squared radial
+ * limit), linearizations: 23 doubles per observation (valid flag, pixel, 2x3 point derivatives,
+ * 2x6 pose derivatives, 2 log-focal derivatives), the layouts the reference's host reads.  The
+ * report is the observation report's shape (evaluate_ms = the kernel).
+ */
+tba_status tba_linearize_inverse_depth(tba_device* device, uint32_t count, const double* measurements,
+                                       size_t measurements_len, double* linearizations, size_t linearizations_len,
+                                       tba_observation_report* report);
+
 #ifdef __cplusplus
 }
 #endif

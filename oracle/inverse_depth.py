@@ -1,0 +1,139 @@
+"""CPU restatement of the reference's inverse-depth geometry (test infrastructure only).
+
+Follows src/geometry/inverse-depth.ts: `initializeInverseDepth` (:19-35) and `inverseDepthJacobian`
+(:38-74), with the CPU projection of src/geometry/camera.ts (`radialLimitSquared` :15-24,
+`cameraProjection` :27-61, `unprojectPixel` :64-105) and the pose helpers of src/geometry/pose.ts
+(`transformPoint` :28-33, `cameraCenter` :34-39).  These are the functions the reference's own test
+compares its device linearisation with (tests/typeshade/inverse-depth-cases.mjs:126-165).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def radial_limit_squared(k1: float, k2: float) -> float:
+    if k2 == 0:
+        return -1 / (3 * k1) if k1 < 0 else math.inf
+    a, b = 5 * k2, 3 * k1
+    d = b * b - 4 * a
+    if d < 0:
+        return math.inf
+    q = -0.5 * (b + (1.0 if b >= 0 else -1.0) * math.sqrt(d))
+    roots = []
+    for x in (q / a, (1 / q) if q != 0 else math.inf):
+        if x > 0 and math.isfinite(x):
+            roots.append(x)
+    return min(roots) if roots else math.inf
+
+
+def camera_projection(k: dict, q):
+    """(pixel, 2x3 jacobian row-major) or None."""
+    X, Y, Z = float(q[0]), float(q[1]), float(q[2])
+    if not Z > 1e-12 or not all(math.isfinite(v) for v in (X, Y, Z)):
+        return None
+    x, y = X / Z, Y / Z
+    r2 = x * x + y * y
+    k1, k2 = k.get("k1") or 0, k.get("k2") or 0
+    if r2 >= radial_limit_squared(k1, k2):
+        return None
+    d = 1 + k1 * r2 + k2 * r2 * r2
+    g = 2 * (k1 + 2 * k2 * r2)
+    xx, xy, yy = d + g * x * x, g * x * y, d + g * y * y
+    if not (d > 0 and 1 + 3 * k1 * r2 + 5 * k2 * r2 * r2 > 0):
+        return None
+    pixel = (k["fx"] * x * d + k["cx"], k["fy"] * y * d + k["cy"])
+    jac = [k["fx"] * xx / Z, k["fx"] * xy / Z, -k["fx"] * (xx * x + xy * y) / Z,
+           k["fy"] * xy / Z, k["fy"] * yy / Z, -k["fy"] * (xy * x + yy * y) / Z]
+    if not all(math.isfinite(v) for v in (*pixel, *jac)):
+        return None
+    return pixel, jac
+
+
+def unproject_pixel(k: dict, pixel):
+    xd, yd = (pixel[0] - k["cx"]) / k["fx"], (pixel[1] - k["cy"]) / k["fy"]
+    rd = math.hypot(xd, yd)
+    if not math.isfinite(rd):
+        return None
+    if rd == 0:
+        return (0.0, 0.0)
+    k1, k2 = k.get("k1") or 0, k.get("k2") or 0
+    limit2 = radial_limit_squared(k1, k2)
+    if math.isfinite(limit2) and rd >= math.sqrt(limit2) * (1 + k1 * limit2 + k2 * limit2 * limit2):
+        return None
+    r = rd
+    for _ in range(50):
+        r2 = r * r
+        d = 1 + k1 * r2 + k2 * r2 * r2
+        slope = 1 + 3 * k1 * r2 + 5 * k2 * r2 * r2
+        if not (slope > 1e-10 and d > 0):
+            return None
+        residual = r * d - rd
+        if abs(residual) <= 1e-12 * max(1, rd):
+            return (xd * r / rd, yd * r / rd)
+        step, accepted = residual / slope, False
+        for _ in range(25):
+            nxt = r - step
+            n2 = nxt * nxt
+            if (nxt >= 0 and n2 < limit2 and 1 + 3 * k1 * n2 + 5 * k2 * n2 * n2 > 0
+                    and abs(nxt * (1 + k1 * n2 + k2 * n2 * n2) - rd) < abs(residual)):
+                r, accepted = nxt, True
+                break
+            step *= 0.5
+        if not accepted:
+            return None
+    return None
+
+
+def transform_point(pose, X):
+    R, t = np.asarray(pose["R"], float).ravel(), np.asarray(pose["t"], float).ravel()
+    return [R[3 * i] * X[0] + R[3 * i + 1] * X[1] + R[3 * i + 2] * X[2] + t[i] for i in range(3)]
+
+
+def camera_center(pose):
+    R, t = np.asarray(pose["R"], float).ravel(), np.asarray(pose["t"], float).ravel()
+    return [-R[i] * t[0] - R[i + 3] * t[1] - R[i + 6] * t[2] for i in range(3)]
+
+
+def initialize_inverse_depth(view: dict, pixel, xyz=None) -> dict:
+    ray = unproject_pixel(view["camera"], pixel)
+    if ray is None:
+        raise ValueError("Inverse-depth anchor cannot be unprojected")
+    params = [ray[0], ray[1], 0.0]
+    if xyz is not None:
+        q = transform_point(view["pose"], xyz)
+        if not (q[2] > 0) or not all(math.isfinite(v) for v in q):
+            raise ValueError("Invalid finite inverse-depth seed")
+        params = [q[0] / q[2], q[1] / q[2], 1 / q[2]]
+    pose = view["pose"]
+    return {"reference": {"R": np.array(pose["R"], float).ravel(), "t": np.array(pose["t"], float).ravel()},
+            "parameters": np.array(params, float)}
+
+
+def inverse_depth_jacobian(camera: dict, pose: dict, point: dict):
+    """{pixel, point (2x3), pose (2x6), focal (2)} or None, in the reference's summation order."""
+    r = np.asarray(point["parameters"], float)
+    Rv, Rr = np.asarray(pose["R"], float).ravel(), np.asarray(point["reference"]["R"], float).ravel()
+    A = [0.0] * 9
+    C = camera_center(point["reference"])
+    T = transform_point(pose, C)
+    for i in range(3):
+        for j in range(3):
+            for k in range(3):
+                A[3 * i + j] += Rv[3 * i + k] * Rr[3 * j + k]
+    q = [A[3 * i] * r[0] + A[3 * i + 1] * r[1] + A[3 * i + 2] + r[2] * T[i] for i in range(3)]
+    proj = camera_projection(camera, q)
+    if proj is None:
+        return None
+    pixel, J = proj
+    pt, cam = [0.0] * 6, [0.0] * 12
+    B = [0, q[2], -q[1], -q[2], 0, q[0], q[1], -q[0], 0]
+    for row in range(2):
+        for col in range(3):
+            for k in range(3):
+                pt[3 * row + col] += J[3 * row + k] * (A[3 * k + col] if col < 2 else T[k])
+                cam[6 * row + col] += J[3 * row + k] * B[3 * k + col]
+            cam[6 * row + col + 3] = r[2] * J[3 * row + col]
+    return {"pixel": pixel, "point": np.array(pt), "pose": np.array(cam),
+            "focal": np.array([pixel[0] - camera["cx"], pixel[1] - camera["cy"]])}

@@ -9,6 +9,8 @@ floating-point operations and random draws, so that the scenes are bit-identical
 * ``joint_focal_fixture``     tests/typeshade/joint-focal-cases.mjs:2-80 (jointFocalFixture)
 * ``scene``                   tests/scene.ts:10-61                       (scene)
 * ``perturbed``               tests/bundle-adjustment.test.ts:7-30       (perturbed)
+* ``inverse_depth_scene``     tests/typeshade/inverse-depth-cases.mjs:1-56  (inverseDepthScene)
+* ``inverse_depth_long_scene`` tests/typeshade/inverse-depth-cases.mjs:58-85 (inverseDepthLongScene)
 
 The reference hashes ``JSON.stringify(input)`` of some of these scenes in its benchmark records
 (docs/experiments/gpu/*.json, ``inputSha256``).  ``js_json`` restates JSON.stringify (ECMAScript
@@ -393,3 +395,57 @@ def perturbed():
         views.append({**v, "pose": {"R": f64(R), "t": f64(t)}})
     landmarks = [{**p, "xyz": f64([x + (rng() - 0.5) * 0.08 for x in p["xyz"]])} for p in reconstruction["landmarks"]]
     return {"views": views, "landmarks": landmarks}
+
+
+def inverse_depth_scene(count=4):
+    """inverseDepthScene (tests/typeshade/inverse-depth-cases.mjs:1-56): `count` views turning about
+    y along a slightly curved path, 25 points 5-7.4 in front, every point seen by every view,
+    pixels projected exactly (k1 = -0.03)."""
+    camera = {"fx": 800, "fy": 760, "cx": 320, "cy": 240, "k1": -0.03}
+    views = []
+    for i in range(count):
+        y = i * 0.07
+        c, s = math.cos(y), math.sin(y)
+        R = f64([c, 0, s, 0, 1, 0, -s, 0, c])
+        C = [i * 0.32, math.sin(i) * 0.04, 0.02 * i * i]
+        t = f64([-R[3 * r] * C[0] - R[3 * r + 1] * C[1] - R[3 * r + 2] * C[2] for r in range(3)])
+        views.append({"id": i, "camera": camera, "pose": {"R": R, "t": t}})
+    points = [[math.sin(i * 1.3), math.cos(i * 1.7) * 0.8, 5 + (i % 7) * 0.4] for i in range(25)]
+
+    def project(v, X):
+        R, t = v["pose"]["R"], v["pose"]["t"]
+        q = [R[3 * r] * X[0] + R[3 * r + 1] * X[1] + R[3 * r + 2] * X[2] + t[r] for r in range(3)]
+        x, y = q[0] / q[2], q[1] / q[2]
+        d = 1 + camera["k1"] * (x * x + y * y)
+        return [camera["fx"] * x * d + camera["cx"], camera["fy"] * y * d + camera["cy"]]
+
+    return {"views": views,
+            "landmarks": [{"trackId": tid, "xyz": f64(xyz),
+                           "observations": [{"viewId": v["id"], "featureId": tid, "pixel": project(v, xyz)}
+                                            for v in views]}
+                          for tid, xyz in enumerate(points)]}
+
+
+def inverse_depth_long_scene(count=24):
+    """inverseDepthLongScene (tests/typeshade/inverse-depth-cases.mjs:58-85): `count` translated views
+    with identity rotation; each run of 4 consecutive views sees its own copy of the first 12 points
+    of inverse_depth_scene."""
+    source = inverse_depth_scene()
+    camera = source["views"][0]["camera"]
+    views = [{"id": i, "camera": camera,
+              "pose": {"R": f64([1, 0, 0, 0, 1, 0, 0, 0, 1]),
+                       "t": f64([-0.03 * i, -0.04 * math.sin(i), -0.02 * math.sin(i * 0.2)])}}
+             for i in range(count)]
+    landmarks = []
+    for start in range(count - 3):
+        for j, p in enumerate(source["landmarks"][:12]):
+            obs = []
+            for v in views[start:start + 4]:
+                q = [x + v["pose"]["t"][k] for k, x in enumerate(p["xyz"])]
+                x, y = q[0] / q[2], q[1] / q[2]
+                d = 1 + camera["k1"] * (x * x + y * y)
+                obs.append({"viewId": v["id"], "featureId": start * 12 + j,
+                            "pixel": [camera["fx"] * x * d + camera["cx"], camera["fy"] * y * d + camera["cy"]]})
+            landmarks.append({"trackId": start * 12 + j, "xyz": p["xyz"], "observations": obs})
+    return {"views": views, "landmarks": landmarks}
+

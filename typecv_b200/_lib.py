@@ -20,7 +20,7 @@ EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_op
            "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc", "tba_batch_max_cameras",
            "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust", "tba_bundle_vjp",
            "tba_evaluate_observations", "tba_scene_create", "tba_scene_destroy", "tba_scene_adjust",
-           "tba_scene_write", "tba_scene_read")
+           "tba_scene_write", "tba_scene_read", "tba_linearize_inverse_depth")
 
 
 class LibraryError(RuntimeError):
@@ -188,6 +188,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tba_scene_write.argtypes = [vp, vp, P(ctypes.c_double), P(ctypes.c_double)]
     lib.tba_scene_read.restype = ctypes.c_int
     lib.tba_scene_read.argtypes = [vp, vp, P(ctypes.c_double), P(ctypes.c_double)]
+    lib.tba_linearize_inverse_depth.restype = ctypes.c_int
+    lib.tba_linearize_inverse_depth.argtypes = [vp, ctypes.c_uint32, P(ctypes.c_double), ctypes.c_size_t,
+                                                P(ctypes.c_double), ctypes.c_size_t, P(ObservationReport)]
     _lib = lib
     return lib
 

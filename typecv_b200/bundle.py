@@ -47,6 +47,9 @@ class ShadeDevice:
         self._handle = ctypes.c_void_p(handle)
         self.ordinal = ordinal
         self.backend = "cuda"
+        # An optional bound on one call's device working set in bytes (the reference device's
+        # workingBytes); None leaves the bound to the device's free memory.
+        self.working_bytes: int | None = None
 
     @classmethod
     def open(cls, ordinal: int = 0) -> "ShadeDevice":

@@ -1563,4 +1563,65 @@ tba_status tba_scene_read(tba_device* d, tba_scene* r, double* poses, double* po
   return TBA_OK;
 }
 
+tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const double* measurements,
+                                       size_t measurements_len, double* linearizations, size_t linearizations_len,
+                                       tba_observation_report* report) {
+  if (!d) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->error.clear();
+  try {
+    if (count && (!measurements || !linearizations)) argument("Invalid inverse-depth arrays: null pointer");
+    if (measurements_len < 34ull * count || linearizations_len < 23ull * count)
+      argument("Invalid inverse-depth arrays: lengths");
+    if (34ull * count > 0xffffffffull) argument("Inverse-depth measurement budget cannot fit the observations");
+    // Values are not checked, as the reference kernel's are not: a row whose projection leaves the
+    // camera model's domain comes back with a zero flag.
+    CUDA_TRY(cudaSetDevice(d->ordinal));
+    const auto wall0 = std::chrono::steady_clock::now();
+    Layout L;
+    const size_t o_in = L.take<double>(34 * size_t(count)), o_out = L.take<double>(23 * size_t(count));
+    if (d->capacity < L.bytes) {
+      if (d->arena) CUDA_TRY(cudaFree(d->arena));
+      d->arena = nullptr;
+      d->capacity = 0;
+      size_t free_bytes = 0, total_bytes = 0;
+      CUDA_TRY(cudaMemGetInfo(&free_bytes, &total_bytes));
+      if (L.bytes > free_bytes) throw Fail{TBA_ERROR_BUDGET, "Inverse-depth measurement budget cannot fit the observations"};
+      CUDA_TRY(cudaMalloc(&d->arena, L.bytes));
+      d->capacity = L.bytes;
+    }
+    double* din = reinterpret_cast<double*>(d->arena + o_in);
+    double* dout = reinterpret_cast<double*>(d->arena + o_out);
+    cudaStream_t s = d->stream;
+    cudaEvent_t e0 = event(d, 0), e1 = event(d, 1), e2 = event(d, 2), e3 = event(d, 3);
+    CUDA_TRY(cudaEventRecord(e0, s));
+    if (count) CUDA_TRY(cudaMemcpyAsync(din, measurements, 34 * sizeof(double) * count, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaEventRecord(e1, s));
+    tba::launch_linearize_inverse_depth(count, din, dout, s);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(e2, s));
+    if (count) CUDA_TRY(cudaMemcpyAsync(linearizations, dout, 23 * sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(e3, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (report) {
+      std::memset(report, 0, sizeof *report);
+      float ms = 0;
+      CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      report->upload_ms = ms;
+      CUDA_TRY(cudaEventElapsedTime(&ms, e1, e2));
+      report->evaluate_ms = ms;
+      CUDA_TRY(cudaEventElapsedTime(&ms, e2, e3));
+      report->download_ms = ms;
+      report->h2d_bytes = 34ull * 8 * count;
+      report->d2h_bytes = 23ull * 8 * count;
+      report->kernel_launches = count ? 1 : 0;
+      report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+    }
+  } catch (const Fail& f) {
+    d->error = f.message;
+    return f.status;
+  }
+  return TBA_OK;
+}
+
 }  // extern "C"

@@ -161,3 +161,79 @@ void launch_observations(const ObsParams& a, cudaStream_t s) {
 }
 
 }  // namespace tba
+
+// ---- inverse-depth linearisation (linearizeInverseDepth, src/sfm/depth/gpu/inverse-depth.shade.ts) ----
+//
+// One observation per thread.  Input row (34 words): the anchored point's parameters a, b, rho
+// (normalised image coordinates and inverse depth in its reference camera), the reference pose
+// (R row-major, t), the observing pose, the observing camera (fx, fy, cx, cy, k1, k2) and its
+// squared radial limit.  Output row (23 words): valid flag, the projected pixel, the pixel's
+// derivatives with respect to (a, b, rho) and to the observing pose's rotation and translation,
+// and with respect to the log of a shared focal scale.  The point in the observing camera is
+// q = a A0 + b A1 + A2 + rho T with A_k the observing rotation applied to the reference rotation's
+// k-th row and T the observing rotation applied to the reference centre plus the observing
+// translation: the point scaled by rho, so its projection is unchanged.
+namespace tba {
+namespace {
+
+__global__ void __launch_bounds__(256) k_linearize_inverse_depth(uint32_t count, const double* __restrict__ in,
+                                                                  double* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const double* m = in + 34 * size_t(i);
+  double* o = out + 23 * size_t(i);
+  for (int k = 0; k < 23; k++) o[k] = 0;
+  const double a = m[0], b = m[1], rho = m[2];
+  double cx = 0, cy = 0, cz = 0;
+  for (int k = 0; k < 3; k++) {
+    cx -= m[3 + 3 * k] * m[12 + k];
+    cy -= m[4 + 3 * k] * m[12 + k];
+    cz -= m[5 + 3 * k] * m[12 + k];
+  }
+  double A0[3], A1[3], A2[3], T[3];
+  for (int row = 0; row < 3; row++) {
+    const double r0 = m[15 + 3 * row], r1 = m[16 + 3 * row], r2 = m[17 + 3 * row];
+    A0[row] = r0 * m[3] + r1 * m[4] + r2 * m[5];
+    A1[row] = r0 * m[6] + r1 * m[7] + r2 * m[8];
+    A2[row] = r0 * m[9] + r1 * m[10] + r2 * m[11];
+    T[row] = (r0 * cx + r1 * cy + r2 * cz) + m[24 + row];
+  }
+  double q[3];
+  for (int r = 0; r < 3; r++) q[r] = a * A0[r] + b * A1[r] + A2[r] + rho * T[r];
+  if (!(q[2] > 0.000000000001)) return;
+  const double x = q[0] / q[2], y = q[1] / q[2], r2 = x * x + y * y;
+  const double fx = m[27], fy = m[28], k1 = m[31], k2 = m[32];
+  if (!(r2 < m[33])) return;
+  const double d = 1. + k1 * r2 + k2 * r2 * r2;
+  if (!(d > 0. && 1. + 3. * k1 * r2 + 5. * k2 * r2 * r2 > 0.)) return;
+  const double g = 2. * (k1 + 2. * k2 * r2);
+  const double xx = d + g * x * x, xy = g * x * y, yy = d + g * y * y;
+  const double J0[3] = {fx * xx / q[2], fx * xy / q[2], -fx * (xx * x + xy * y) / q[2]};
+  const double J1[3] = {fy * xy / q[2], fy * yy / q[2], -fy * (xy * x + yy * y) / q[2]};
+  o[0] = 1.;
+  o[1] = fx * x * d + m[29];
+  o[2] = fy * y * d + m[30];
+  for (int row = 0; row < 2; row++) {
+    const double* J = row == 0 ? J0 : J1;
+    o[3 + row * 3] = J[0] * A0[0] + J[1] * A0[1] + J[2] * A0[2];
+    o[4 + row * 3] = J[0] * A1[0] + J[1] * A1[1] + J[2] * A1[2];
+    o[5 + row * 3] = J[0] * T[0] + J[1] * T[1] + J[2] * T[2];
+    double* at = o + 9 + row * 6;
+    at[0] = -J[1] * q[2] + J[2] * q[1];
+    at[1] = J[0] * q[2] - J[2] * q[0];
+    at[2] = -J[0] * q[1] + J[1] * q[0];
+    at[3] = rho * J[0];
+    at[4] = rho * J[1];
+    at[5] = rho * J[2];
+  }
+  o[21] = fx * x * d;
+  o[22] = fy * y * d;
+}
+
+}  // namespace
+
+void launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s) {
+  if (count) k_linearize_inverse_depth<<<(count + 255) / 256, 256, 0, s>>>(count, in, out);
+}
+
+}  // namespace tba
