@@ -5,6 +5,13 @@ Follows src/geometry/inverse-depth.ts: `initializeInverseDepth` (:19-35) and `in
 `cameraProjection` :27-61, `unprojectPixel` :64-105) and the pose helpers of src/geometry/pose.ts
 (`transformPoint` :28-33, `cameraCenter` :34-39).  These are the functions the reference's own test
 compares its device linearisation with (tests/typeshade/inverse-depth-cases.mjs:126-165).
+
+`bundle_adjust_inverse_depth` is the reference's CPU `bundleAdjustInverseDepth`
+(src/sfm/depth/inverse-depth-bundle.ts:717-729): the same host steps as the device operator (the
+reference shares `inverseDepthBundleSteps` between its two arms, so the steps here are the
+package's), answered with this file's CPU linearisation.  `fit_inverse_depth` restates
+`fitInverseDepth` (src/geometry/inverse-depth.ts:184-249) with `solveSystem`
+(src/geometry/numerics.ts:71-100), which the reference's bundle tests use as the fixed-pose baseline.
 """
 from __future__ import annotations
 
@@ -137,3 +144,89 @@ def inverse_depth_jacobian(camera: dict, pose: dict, point: dict):
             cam[6 * row + col + 3] = r[2] * J[3 * row + col]
     return {"pixel": pixel, "point": np.array(pt), "pose": np.array(cam),
             "focal": np.array([pixel[0] - camera["cx"], pixel[1] - camera["cy"]])}
+
+
+def linearize_job(job):
+    """linearizeInverseDepthJob (src/sfm/depth/inverse-depth-bundle.ts:717-719)."""
+    return [inverse_depth_jacobian(m["view"]["camera"], m["view"]["pose"], m["point"]) for m in job["measurements"]]
+
+
+def bundle_adjust_inverse_depth(inp, constraints=(), options=None):
+    from typecv_b200.inverse_depth_bundle import drive, inverse_depth_bundle_steps
+    return drive(inverse_depth_bundle_steps(inp, constraints, options), linearize_job)
+
+
+def solve_system(matrix, rhs):
+    n = len(rhs)
+    a = [[float(matrix[i * n + j]) for j in range(n)] + [float(rhs[i])] for i in range(n)]
+    if any(not all(math.isfinite(v) for v in row) for row in a):
+        return None
+    scale = max([0.0] + [max(abs(v) for v in row[:n]) for row in a])
+    if not scale > 0:
+        return [] if n == 0 else None
+    for j in range(n):
+        p = j
+        for i in range(j + 1, n):
+            if abs(a[i][j]) > abs(a[p][j]):
+                p = i
+        if abs(a[p][j]) < 1e-14 * scale:
+            return None
+        a[p], a[j] = a[j], a[p]
+        for i in range(j + 1, n):
+            f = a[i][j] / a[j][j]
+            for k in range(j, n + 1):
+                a[i][k] -= f * a[j][k]
+    out = [0.0] * n
+    for i in range(n - 1, -1, -1):
+        b = a[i][n]
+        for j in range(i + 1, n):
+            b -= a[i][j] * out[j]
+        out[i] = b / a[i][i]
+    return out if all(math.isfinite(v) for v in out) else None
+
+
+def fit_inverse_depth(observations, iterations=12, sigma=1.0, huber=3.0):
+    """observations: [{camera, pose, pixel}], the first one the anchor."""
+    from typecv_b200.inverse_depth import inverse_depth_covariance
+    point = initialize_inverse_depth({"camera": observations[0]["camera"], "pose": observations[0]["pose"]},
+                                     observations[0]["pixel"])
+    lam = 1e-3
+
+    def linearize(p):
+        H, b = [0.0] * 9, [0.0] * 3
+        cost = 0.0
+        for o in observations:
+            j = inverse_depth_jacobian(o["camera"], o["pose"], p)
+            if j is None:
+                return None
+            r = (j["pixel"][0] - o["pixel"][0], j["pixel"][1] - o["pixel"][1])
+            e = math.hypot(*r)
+            w = (1 if e <= huber else huber / e) / sigma ** 2
+            cost += e * e if e <= huber else 2 * huber * e - huber * huber
+            for row in range(2):
+                for k in range(3):
+                    b[k] -= w * j["point"][3 * row + k] * r[row]
+                    for l in range(3):
+                        H[3 * k + l] += w * j["point"][3 * row + k] * j["point"][3 * row + l]
+        return {"H": H, "b": b, "cost": cost}
+
+    current = linearize(point)
+    for _ in range(iterations):
+        if current is None:
+            break
+        H = list(current["H"])
+        for k in range(3):
+            H[4 * k] += lam * max(H[4 * k], 1e-10)
+        d = solve_system(H, current["b"])
+        if d is None:
+            break
+        candidate = {**point, "parameters": np.array([x + d[k] for k, x in enumerate(point["parameters"])])}
+        nxt = linearize(candidate)
+        if nxt is not None and nxt["cost"] < current["cost"]:
+            point, current = candidate, nxt
+            lam /= 3
+        else:
+            lam *= 10
+    if current is None:
+        raise ValueError("Invalid inverse-depth observations")
+    return {"point": point, "covariance": inverse_depth_covariance(current["H"])}

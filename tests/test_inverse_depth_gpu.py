@@ -113,3 +113,35 @@ def test_long_scene_in_tail_batches(device):
     assert len(measurements) == 1008 and out["batches"] == 8 and out["batchSize"] == 127
     assert all(r is not None for r in out["rows"])
     assert compare(measurements, out["rows"]) <= 1e-8
+
+
+def test_joint_bundle_on_the_device_matches_the_cpu_arm(device):
+    """inverseDepthGpuCases' joint half (inverse-depth-cases.mjs:166-184)."""
+    from typecv_b200.inverse_depth_bundle import bundle_adjust_inverse_depth_gpu
+    model = inverse_depth_scene()
+    cpu = oid.bundle_adjust_inverse_depth(model, [], {"iterations": 1})
+    gpu = bundle_adjust_inverse_depth_gpu(device, model, [], {"iterations": 1, "solver": "sparse",
+                                                              "measurementBatchSize": 31})
+    assert cpu["uncertainty"]["observable"] and gpu["uncertainty"]["observable"]
+    for a, b in zip(cpu["estimates"], gpu["estimates"]):
+        assert abs(a["covariance"][8] - b["covariance"][8]) / a["covariance"][8] <= 1e-6
+    d = gpu["diagnostics"]
+    assert d["backend"] == "cuda-jacobians/host-f64-Schur"
+    assert d["measurementBatchSize"] == 31 and d["measurementBatches"] == 2 * 4
+    assert d["kernelLaunches"] == d["measurementBatches"] + d["costBatches"]
+
+
+def test_large_sparse_joint_solve_in_tail_batches(device):
+    """inverseDepthLargeGpuCase (inverse-depth-cases.mjs:87-123)."""
+    from typecv_b200.inverse_depth_bundle import bundle_adjust_inverse_depth_gpu
+    model = inverse_depth_long_scene()
+    cpu = oid.bundle_adjust_inverse_depth(model, [], {"iterations": 1, "solver": "sparse"})
+    gpu = bundle_adjust_inverse_depth_gpu(device, model, [], {"iterations": 1, "solver": "sparse",
+                                                              "measurementBatchSize": 127})
+    assert cpu["uncertainty"]["observable"] and gpu["uncertainty"]["observable"]
+    worst = max(abs(b["covariance"][8] / a["covariance"][8] - 1) for a, b in zip(cpu["estimates"], gpu["estimates"]))
+    assert worst <= 1e-4
+    d = gpu["diagnostics"]
+    assert d["cameraParameters"] > 96 and d["linearSolver"] == "sparse" and gpu["uncertainty"]["poses"] == "joint"
+    assert d["measurementBatches"] == 16
+    assert abs(d["finalCost"] - cpu["diagnostics"]["finalCost"]) <= 1e-9 * max(1.0, cpu["diagnostics"]["finalCost"])

@@ -120,3 +120,177 @@ def linearize_inverse_depth_gpu(device: ShadeDevice, job: dict, batch_size: int 
     """linearizeInverseDepthGpu (inverse-depth.ts:108-114): one linearisation or None per measurement,
     in order."""
     return linearize_batches(device, job, batch_size)["rows"]
+
+
+# ---- host geometry of the anchored inverse-depth chart (src/geometry/inverse-depth.ts, pose.ts) ----
+
+def multiply3(a, b) -> list[float]:
+    """multiply (src/geometry/linear.ts:8-17) for 3x3, row-major, sums in index order."""
+    out = []
+    for r in range(3):
+        for c in range(3):
+            s = 0.0
+            for k in range(3):
+                s += a[r * 3 + k] * b[k * 3 + c]
+            out.append(s)
+    return out
+
+
+def rotation_exp(w) -> list[float]:
+    """rotationExp (src/geometry/pose.ts:40-51)."""
+    x, y, z = (float(v) for v in w[:3])
+    if not all(math.isfinite(v) for v in (x, y, z)):
+        raise RangeError("Invalid rotation vector")
+    theta = math.hypot(x, y, z)
+    a = 1 - theta * theta / 6 if theta < 1e-7 else math.sin(theta) / theta
+    b = 0.5 - theta * theta / 24 if theta < 1e-7 else (1 - math.cos(theta)) / (theta * theta)
+    W = [0.0, -z, y, z, 0.0, -x, -y, x, 0.0]
+    W2 = multiply3(W, W)
+    return [(1 if i % 4 == 0 else 0) + a * W[i] + b * W2[i] for i in range(9)]
+
+
+def transform_point(pose, X) -> list[float]:
+    """transformPoint (src/geometry/pose.ts:28-33)."""
+    R, t = pose["R"], pose["t"]
+    return [float(R[i * 3]) * X[0] + float(R[i * 3 + 1]) * X[1] + float(R[i * 3 + 2]) * X[2] + float(t[i])
+            for i in range(3)]
+
+
+def camera_center(pose) -> list[float]:
+    """cameraCenter (src/geometry/pose.ts:34-39)."""
+    R, t = pose["R"], pose["t"]
+    return [-float(R[i]) * float(t[0]) - float(R[i + 3]) * float(t[1]) - float(R[i + 6]) * float(t[2]) for i in range(3)]
+
+
+def update_pose(pose, delta) -> dict:
+    """updatePose (src/geometry/pose.ts:52-57): left rotation, additive camera translation."""
+    dR = rotation_exp(delta)
+    rotated = transform_point({"R": dR, "t": [0.0, 0.0, 0.0]}, [float(v) for v in pose["t"]])
+    return {"R": np.array(multiply3(dR, [float(v) for v in pose["R"]])),
+            "t": np.array([rotated[i] + delta[i + 3] for i in range(3)])}
+
+
+def validate_pose(p) -> None:
+    """validatePose (src/geometry/pose.ts:13-27)."""
+    R, t = np.asarray(p["R"], float).ravel(), np.asarray(p["t"], float).ravel()
+    if R.size != 9 or t.size != 3 or not (np.all(np.isfinite(R)) and np.all(np.isfinite(t))):
+        raise RangeError("Invalid pose dimensions or values")
+    q = multiply3(list(R), [R[0], R[3], R[6], R[1], R[4], R[7], R[2], R[5], R[8]])
+    det = (R[0] * (R[4] * R[8] - R[5] * R[7]) - R[1] * (R[3] * R[8] - R[5] * R[6])
+           + R[2] * (R[3] * R[7] - R[4] * R[6]))
+    if any(abs(v - (1 if i % 4 == 0 else 0)) > 1e-6 for i, v in enumerate(q)) or abs(det - 1) > 1e-6:
+        raise RangeError("Pose rotation must belong to SO(3)")
+
+
+def validate_camera(k) -> None:
+    """validateCamera (src/geometry/camera.ts:5-12)."""
+    vals = [k["fx"], k["fy"], k["cx"], k["cy"], k.get("k1") or 0, k.get("k2") or 0]
+    if not all(math.isfinite(v) for v in vals) or k["fx"] <= 0 or k["fy"] <= 0:
+        raise RangeError("Invalid camera: finite parameters and positive focal lengths required")
+
+
+def unproject_pixel(k, pixel):
+    """unprojectPixel (src/geometry/camera.ts:64-105): the normalised bearing of a pixel on the
+    radial model's monotone branch, by backtracking Newton steps; None when it has none."""
+    validate_camera(k)
+    xd, yd = (pixel[0] - k["cx"]) / k["fx"], (pixel[1] - k["cy"]) / k["fy"]
+    rd = math.hypot(xd, yd)
+    if not math.isfinite(rd):
+        return None
+    if rd == 0:
+        return (0.0, 0.0)
+    k1, k2 = k.get("k1") or 0, k.get("k2") or 0
+    limit2 = radial_limit_squared(k1, k2)
+    if math.isfinite(limit2) and rd >= math.sqrt(limit2) * (1 + k1 * limit2 + k2 * limit2 * limit2):
+        return None
+    r = rd
+    for _ in range(50):
+        r2 = r * r
+        d = 1 + k1 * r2 + k2 * r2 * r2
+        slope = 1 + 3 * k1 * r2 + 5 * k2 * r2 * r2
+        if not (slope > 1e-10 and d > 0):
+            return None
+        residual = r * d - rd
+        if abs(residual) <= 1e-12 * max(1, rd):
+            return (xd * r / rd, yd * r / rd)
+        step, accepted = residual / slope, False
+        for _ in range(25):
+            nxt = r - step
+            n2 = nxt * nxt
+            if (nxt >= 0 and n2 < limit2 and 1 + 3 * k1 * n2 + 5 * k2 * n2 * n2 > 0
+                    and abs(nxt * (1 + k1 * n2 + k2 * n2 * n2) - rd) < abs(residual)):
+                r, accepted = nxt, True
+                break
+            step *= 0.5
+        if not accepted:
+            return None
+    return None
+
+
+def initialize_inverse_depth(view: dict, pixel, xyz=None) -> dict:
+    """initializeInverseDepth (src/geometry/inverse-depth.ts:19-35): the chart anchored at the
+    view, (a, b) the pixel's bearing and rho the inverse depth of xyz (0 without it)."""
+    validate_camera(view["camera"])
+    validate_pose(view["pose"])
+    ray = unproject_pixel(view["camera"], pixel)
+    if ray is None:
+        raise RangeError("Inverse-depth anchor cannot be unprojected")
+    params = [ray[0], ray[1], 0.0]
+    if xyz is not None:
+        q = transform_point(view["pose"], [float(v) for v in xyz])
+        if not q[2] > 0 or not all(math.isfinite(v) for v in q):
+            raise RangeError("Invalid finite inverse-depth seed")
+        params = [q[0] / q[2], q[1] / q[2], 1 / q[2]]
+    return {"reference": {"R": np.array(view["pose"]["R"], float).ravel(), "t": np.array(view["pose"]["t"], float).ravel()},
+            "parameters": np.array(params, float)}
+
+
+def inverse3(a) -> list[float] | None:
+    """inverse3 (src/geometry/numerics.ts:103-131): adjugate over the determinant."""
+    a00, a01, a02, a10, a11, a12, a20, a21, a22 = (float(v) for v in a)
+    c00, c01, c02 = a11 * a22 - a12 * a21, a02 * a21 - a01 * a22, a01 * a12 - a02 * a11
+    det = a00 * c00 + a10 * c01 + a20 * c02
+    if not math.isfinite(det) or det == 0:
+        return None
+    out = [c00 / det, c01 / det, c02 / det, (a12 * a20 - a10 * a22) / det, (a00 * a22 - a02 * a20) / det,
+           (a02 * a10 - a00 * a12) / det, (a10 * a21 - a11 * a20) / det, (a01 * a20 - a00 * a21) / det,
+           (a00 * a11 - a01 * a10) / det]
+    return out if all(math.isfinite(v) for v in out) else None
+
+
+def inverse_depth_covariance(information) -> list[float] | None:
+    """inverseDepthCovariance (src/geometry/inverse-depth.ts:157-164): the inverse of a 3x3
+    information matrix through its diagonally scaled form; None where it is not observable."""
+    info = [float(v) for v in information]
+    diagonal = [math.sqrt(info[i]) if info[i] >= 0 else math.nan for i in (0, 4, 8)]
+    if any(not (x > 0 and math.isfinite(x)) for x in diagonal):
+        return None
+    scaled = [x / (diagonal[i // 3] * diagonal[i % 3]) for i, x in enumerate(info)]
+    inv = inverse3(scaled)
+    if inv is None or any(not inv[i] > 0 for i in (0, 4, 8)):
+        return None
+    return [x / (diagonal[i // 3] * diagonal[i % 3]) for i, x in enumerate(inv)]
+
+
+def inverse_depth_point(p) -> np.ndarray | None:
+    """inverseDepthPoint (src/geometry/inverse-depth.ts:77-87): the world point, for rho > 0."""
+    a, b, rho = (float(v) for v in p["parameters"])
+    if not rho > 0:
+        return None
+    C = camera_center(p["reference"])
+    R = p["reference"]["R"]
+    X = np.array([C[i] + (float(R[i]) * a + float(R[3 + i]) * b + float(R[6 + i])) / rho for i in range(3)])
+    return X if np.all(np.isfinite(X)) else None
+
+
+def rescale_inverse_depth(p, scale: float, origin) -> dict:
+    """rescaleInverseDepth (src/geometry/inverse-depth.ts:133-154) without a covariance: the chart of
+    the same bearing after the map is scaled about `origin`."""
+    if not (scale > 0 and math.isfinite(scale)):
+        raise RangeError("Invalid inverse-depth map scale")
+    C = [origin[i] + scale * (c - origin[i]) for i, c in enumerate(camera_center(p["reference"]))]
+    R = np.array(p["reference"]["R"], float)
+    t = np.array([-R[3 * i] * C[0] - R[3 * i + 1] * C[1] - R[3 * i + 2] * C[2] for i in range(3)])
+    parameters = np.array(p["parameters"], float)
+    parameters[2] /= scale
+    return {"reference": {"R": R, "t": t}, "parameters": parameters}
