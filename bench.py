@@ -15,7 +15,9 @@ the timed region).  The working set (~1.5 GB) is larger than the 126 MB L2, so n
 library records around every product launch.
 
 ``--config cfg3`` runs the batched local-window solve (512 arc windows, one persistent launch) and
-``--config cfg4`` the adjoint of a 200-camera / 50k-point solve; each prints its own line.
+``--config cfg4`` the adjoint of a 200-camera / 50k-point solve; ``--config invdepth`` the
+inverse-depth measurement linearisation (4M seeded measurements per call, ``tba_linearize_inverse_depth``);
+each prints its own line.
 
 Multi-GPU runs are replicas (the operator does not shard): each rank solves its own copy of the
 scene, no collective touches the data path, and ``scaling`` is "weak".
@@ -51,7 +53,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="cfg2", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--config", default="cfg2", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "invdepth"])
     ap.add_argument("--iterations", type=int, default=None, help="LM iterations per step")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -228,8 +230,45 @@ def finish_dist(world):
         dist.destroy_process_group()
 
 
+def invdepth_cpu(rows):
+    """The oracle's C++ CPU linearisation (the reference's inverseDepthJacobian, OpenMP over the host
+    cores) over `rows`: (seconds, output rows, threads)."""
+    from oracle import inverse_depth as oid
+    oid.linearize_rows(rows[:16])
+    t0 = time.perf_counter()
+    out = oid.linearize_rows(rows)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return time.perf_counter() - t0, out, threads
+
+
+INVDEPTH_METRIC = "inverse-depth measurement linearisations/s, 1 B200"
+INVDEPTH_UNIT = "measurements/s"
+INVDEPTH_ROWS = 4 << 20
+
+
 def run_reference(args, world, rank):
     if rank != 0:
+        return
+    if args.config == "invdepth":
+        from typecv_b200 import synthetic as S
+        rows = S.inverse_depth_rows(measurements=max(1, int(INVDEPTH_ROWS * args.scale)))
+        for _ in range(args.warmup):
+            invdepth_cpu(rows[:4096])
+        total, threads = 0.0, 1
+        for _ in range(args.steps):
+            dt, _, threads = invdepth_cpu(rows)
+            total += dt
+        value = len(rows) * args.steps / total
+        line = {"metric": INVDEPTH_METRIC, "value": value, "unit": INVDEPTH_UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded)",
+                "config": {"workload": f"invdepth: {len(rows)} inverse-depth measurement rows"}, "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": INVDEPTH_UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"all {len(rows)} rows per step through the CPU inverseDepthJacobian "
+                                           "restated in C++ (oracle/ba_oracle.cpp)"},
+                "e2e": {"value": value, "unit": INVDEPTH_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     cfg = args.config if args.config in ("cfg0", "cfg1", "cfg2") else "cfg2"
     scene = make_scene(cfg, args.scale)
@@ -544,6 +583,82 @@ def run_adjoint(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_inverse_depth(args, world, rank, local):
+    """Row f4: one tba_linearize_inverse_depth call over 4M seeded measurement rows per step (scaled
+    by --scale), pinned host buffers.  ``value`` from the kernel's CUDA events, ``e2e`` from the
+    call's wall time (host-to-device copy of the rows, the kernel, the read of the results)."""
+    import torch
+    import ctypes
+    import typecv_b200 as tb
+    from typecv_b200 import _lib
+    from typecv_b200 import synthetic as S
+    M = max(1, int(INVDEPTH_ROWS * args.scale))
+    rows = S.inverse_depth_rows(measurements=M)
+    src = torch.empty(34 * M, dtype=torch.float64, pin_memory=True).numpy()
+    src[:] = rows.ravel()
+    dst = torch.empty(23 * M, dtype=torch.float64, pin_memory=True).numpy()
+    lib = _lib.load()
+    dev = tb.ShadeDevice.open(local)
+
+    def call():
+        rep = _lib.ObservationReport()
+        st = lib.tba_linearize_inverse_depth(dev.handle, M, _lib.dptr(src), src.size, _lib.dptr(dst), dst.size,
+                                             ctypes.byref(rep))
+        if st != _lib.TBA_OK:
+            raise RuntimeError(lib.tba_last_error(dev.handle).decode())
+        return rep.as_dict()
+
+    try:
+        for _ in range(max(3, args.warmup)):
+            call()
+        reps, walls = [], []
+        barrier(world)
+        with Clocks(local) as clocks:
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                reps.append(call())
+                walls.append(time.perf_counter() - t0)
+            barrier(world)
+    finally:
+        dev.close()
+    kernel_s = max_over_ranks(world, sum(r["evaluate_ms"] for r in reps) / 1000)
+    wall_s = max_over_ranks(world, sum(walls))
+    if rank != 0:
+        return
+    # Every row against the oracle (flags equal, values within 1e-8 of max(1, |value|)).
+    dt, want, threads = invdepth_cpu(rows)
+    got = dst.reshape(M, 23)
+    flags_equal = bool(np.array_equal(want[:, 0], got[:, 0]))
+    ok = want[:, 0] == 1
+    worst = float(np.max(np.abs(want[ok] - got[ok]) / np.maximum(1, np.abs(want[ok])))) if ok.any() else 0.0
+    invalid = int(M - ok.sum())
+    pk, kind = peaks()
+    per_launch_s = kernel_s / args.steps
+    achieved = 456 * M / per_launch_s / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = {"value": M / dt, "unit": INVDEPTH_UNIT, "cores": threads, "kind": "port",
+               "sample": f"all {M} rows through the CPU inverseDepthJacobian restated in C++ "
+                         "(oracle/ba_oracle.cpp, OpenMP)"}
+    line = {"metric": INVDEPTH_METRIC, "value": world * M * args.steps / kernel_s, "unit": INVDEPTH_UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": 1000 * kernel_s / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"invdepth: {M} inverse-depth measurement rows (34 words in, 23 out), "
+                                   "512 ring cameras, one call per step",
+                       "l2": "working set (1.9 GB at 4M rows) larger than L2"},
+            "e2e": {"value": world * M * args.steps / wall_s, "unit": INVDEPTH_UNIT,
+                    "h2d_bytes_per_step": int(reps[-1]["h2d_bytes"]), "d2h_bytes_per_step": int(reps[-1]["d2h_bytes"]),
+                    "upload_ms": reps[-1]["upload_ms"], "download_ms": reps[-1]["download_ms"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                         "note": f"k_linearize_inverse_depth, 456 algorithmic bytes per measurement; peak of {kind}"},
+            "parity": {"rows_checked": M, "flags_equal": flags_equal, "max_rel_vs_oracle": worst,
+                       "invalid_rows": invalid},
+            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": sum(r["kernel_launches"] for r in reps)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = init_dist(args)
@@ -554,6 +669,8 @@ def main():
             run_batch(args, world, rank, local)
         elif args.config == "cfg4":
             run_adjoint(args, world, rank, local)
+        elif args.config == "invdepth":
+            run_inverse_depth(args, world, rank, local)
         else:
             run_single(args, world, rank, local)
     finally:

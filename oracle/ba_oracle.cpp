@@ -15,7 +15,12 @@
 //      joint-focal.shade.ts (K21), resident (one window), with the host's stall monitor.
 //      Its output array has the layout of the reference's `packBundleResult`.
 //
-// Both are compiled with -ffp-contract=off and no FMA so that every product and sum rounds the
+//  (3) `oracle_linearize_inverse_depth`: the reference's CPU `inverseDepthJacobian`
+//      (src/geometry/inverse-depth.ts:38-74, with cameraProjection and radialLimitSquared of
+//      src/geometry/camera.ts:15-61) over rows in the device's 34-word layout, written in the
+//      device's 23-word layout: the checker and CPU baseline of the inverse-depth linearisation.
+//
+// All are compiled with -ffp-contract=off and no FMA so that every product and sum rounds the
 // way the reference's JavaScript does.  Parity is pinned by tests/golden (see tests/).  The
 // operator's per-point, per-observation and per-camera-row loops run under OpenMP: their
 // iterations are independent, so every value is the same as in a serial run.
@@ -1484,3 +1489,56 @@ void oracle_metrics(const oracle_control* ctl, const double* scene, const uint32
 }
 
 }  // extern "C"
+
+// =================================================================================================
+// (3) Inverse-depth linearisation on the CPU (inverseDepthJacobian), one row per measurement.
+namespace {
+
+void inverse_depth_row(const double* m, double* o) {
+  for (int k = 0; k < 23; k++) o[k] = 0;
+  const double* Rr = m + 3;
+  const double* tr = m + 12;
+  const double* Rv = m + 15;
+  const double* tv = m + 24;
+  double C[3], T[3], A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, q[3];
+  for (int i = 0; i < 3; i++) C[i] = -Rr[i] * tr[0] - Rr[i + 3] * tr[1] - Rr[i + 6] * tr[2];
+  for (int i = 0; i < 3; i++) T[i] = Rv[i * 3] * C[0] + Rv[i * 3 + 1] * C[1] + Rv[i * 3 + 2] * C[2] + tv[i];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      for (int k = 0; k < 3; k++) A[3 * i + j] += Rv[3 * i + k] * Rr[3 * j + k];
+  for (int i = 0; i < 3; i++) q[i] = A[3 * i] * m[0] + A[3 * i + 1] * m[1] + A[3 * i + 2] + m[2] * T[i];
+  const Camera cam_k{m[27], m[28], m[29], m[30], m[31], m[32]};
+  double pixel[2], J[6];
+  if (!camera_projection(cam_k, q, pixel, J)) return;
+  const double B[9] = {0, q[2], -q[1], -q[2], 0, q[0], q[1], -q[0], 0};
+  double point[6] = {0, 0, 0, 0, 0, 0}, cam[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int row = 0; row < 2; row++)
+    for (int col = 0; col < 3; col++) {
+      for (int k = 0; k < 3; k++) {
+        point[3 * row + col] += J[3 * row + k] * (col < 2 ? A[3 * k + col] : T[k]);
+        cam[6 * row + col] += J[3 * row + k] * B[3 * k + col];
+      }
+      cam[6 * row + col + 3] = m[2] * J[3 * row + col];
+    }
+  o[0] = 1;
+  o[1] = pixel[0];
+  o[2] = pixel[1];
+  for (int k = 0; k < 6; k++) o[3 + k] = point[k];
+  for (int k = 0; k < 12; k++) o[9 + k] = cam[k];
+  o[21] = pixel[0] - cam_k.cx;
+  o[22] = pixel[1] - cam_k.cy;
+}
+
+}  // namespace
+
+extern "C" {
+
+// in: n rows of 34 doubles (a, b, rho; reference pose R, t; observing pose R, t; fx, fy, cx, cy,
+// k1, k2; the squared radial limit, unused here: the CPU projection derives it), out: n rows of 23.
+void oracle_linearize_inverse_depth(uint32_t n, const double* in, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < int64_t(n); i++) inverse_depth_row(in + 34 * i, out + 23 * i);
+}
+
+}  // extern "C"
+

@@ -70,6 +70,8 @@ def lib():
         _lib.oracle_gpu_operator.restype = ctypes.c_int
         _lib.oracle_gpu_operator.argtypes = [P(Control), P(ctypes.c_double), P(ctypes.c_uint32),
                                              P(ctypes.c_double)]
+        _lib.oracle_linearize_inverse_depth.restype = None
+        _lib.oracle_linearize_inverse_depth.argtypes = [ctypes.c_uint32, P(ctypes.c_double), P(ctypes.c_double)]
         _lib.oracle_metrics.restype = None
         _lib.oracle_metrics.argtypes = [P(Control), P(ctypes.c_double), P(ctypes.c_uint32), P(ctypes.c_double)]
     return _lib

@@ -146,6 +146,17 @@ def inverse_depth_jacobian(camera: dict, pose: dict, point: dict):
             "focal": np.array([pixel[0] - camera["cx"], pixel[1] - camera["cy"]])}
 
 
+def linearize_rows(rows: np.ndarray) -> np.ndarray:
+    """The C++ restatement of inverseDepthJacobian (oracle/ba_oracle.cpp, OpenMP over the host
+    cores) over (n x 34) rows; (n x 23) rows in the device layout, flag 0 where invalid."""
+    from oracle import bundle_adjust as ob
+    rows = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 34)
+    out = np.zeros((len(rows), 23))
+    if len(rows):
+        ob.lib().oracle_linearize_inverse_depth(len(rows), ob._dptr(rows), ob._dptr(out))
+    return out
+
+
 def linearize_job(job):
     """linearizeInverseDepthJob (src/sfm/depth/inverse-depth-bundle.ts:717-719)."""
     return [inverse_depth_jacobian(m["view"]["camera"], m["view"]["pose"], m["point"]) for m in job["measurements"]]

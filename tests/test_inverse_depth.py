@@ -150,3 +150,23 @@ def test_batch_controls_are_checked_before_any_device_work():
         ID.linearize_batches(small, job)
     assert ID.linearize_batches(NoDevice(), {"measurements": []}) == {"rows": [], "batches": 0, "batchSize": 0,
                                                                       "reports": []}
+
+
+def test_cpp_restatement_is_bit_identical_to_the_python_one():
+    """oracle_linearize_inverse_depth (ba_oracle.cpp, no FMA) against inverse_depth_jacobian on the
+    fixture's measurements, rows outside the model's domain included."""
+    model = inverse_depth_scene()
+    wide = {**model["views"][1], "camera": {"fx": 800, "fy": 760, "cx": 320, "cy": 240, "k1": -10.0}}
+    ms = [{"view": v, "point": anchored(model, track=t, rho=rho)} for t in (0, 7, 13) for rho in (0, 0.2, -5)
+          for v in model["views"] + [wide]]
+    rows = ID.pack_measurements(ms).reshape(-1, 34)
+    out = oid.linearize_rows(rows)
+    invalid = 0
+    for m, r in zip(ms, out):
+        p = oid.inverse_depth_jacobian(m["view"]["camera"], m["view"]["pose"], m["point"])
+        if p is None:
+            invalid += 1
+            assert not r.any()
+            continue
+        assert np.array_equal(np.concatenate([[1], p["pixel"], p["point"], p["pose"], p["focal"]]), r)
+    assert 0 < invalid < len(ms)

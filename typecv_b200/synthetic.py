@@ -14,6 +14,9 @@ camera record (fx, fy, cx, cy, k1, k2; src/contracts/camera-record.ts:12-38).
                     Gaussians in a ball, geometric track lengths (config 2).
 * ``arc_scene``     a local window: cameras on an arc of the ring facing the origin, tracks of
                     2-10 of the nearest cameras (``batch_scenes``: the 512 windows of config 3).
+* ``inverse_depth_rows`` inverse-depth measurements packed as the 34-word rows of
+                    ``tba_linearize_inverse_depth``: points anchored in a ring camera, each seen by
+                    one of the next cameras of the ring.
 
 Every scene then gets Gaussian pixel noise, uniform in-image outliers and a perturbed
 initialisation (rotation by an axis-angle of fixed size, translation by a fraction of its norm,
@@ -311,3 +314,32 @@ CONFIGS = {
     "cfg1": lambda: helix_scene(),
     "cfg2": lambda: sphere_scene(),
 }
+
+
+def inverse_depth_rows(seed=5, measurements=4 << 20, cameras=512, radius=5.0, cube=2.0, reach=8) -> np.ndarray:
+    """(measurements x 34) rows: a point uniform in a cube about the origin, anchored in a ring camera
+    (a, b the normalised bearing, rho the inverse depth), observed by one of the `reach` cameras that
+    follow its anchor on the ring; the cameras carry the intrinsics of ``intrinsics`` and their
+    squared radial limit."""
+    rng = np.random.default_rng(seed)
+    angles = np.arange(cameras) * (2 * np.pi / cameras)
+    centers = np.stack([radius * np.cos(angles), radius * np.sin(angles), 0.3 * np.sin(3 * angles)], axis=1)
+    poses = poses_from(look_at(centers, np.zeros((cameras, 3))), centers)
+    K = intrinsics(cameras)
+    k1 = K[:, 4]
+    limit = np.where(k1 < 0, -1 / (3 * np.where(k1 < 0, k1, -1)), 1e30)
+    ref = rng.integers(0, cameras, measurements)
+    obs = (ref + rng.integers(1, reach + 1, measurements)) % cameras
+    X = rng.uniform(-cube / 2, cube / 2, (measurements, 3))
+    R = poses[ref, :9].reshape(-1, 3, 3)
+    q = np.einsum("nij,nj->ni", R, X) + poses[ref, 9:]
+    rows = np.empty((measurements, 34))
+    rows[:, 0] = q[:, 0] / q[:, 2]
+    rows[:, 1] = q[:, 1] / q[:, 2]
+    rows[:, 2] = 1 / q[:, 2]
+    rows[:, 3:15] = poses[ref]
+    rows[:, 15:27] = poses[obs]
+    rows[:, 27:33] = K[obs, :6]
+    rows[:, 33] = limit[obs]
+    return rows
+
