@@ -1597,8 +1597,7 @@ tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const doub
     CUDA_TRY(cudaEventRecord(e0, s));
     if (count) CUDA_TRY(cudaMemcpyAsync(din, measurements, 34 * sizeof(double) * count, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaEventRecord(e1, s));
-    tba::launch_linearize_inverse_depth(count, din, dout, s);
-    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(tba::launch_linearize_inverse_depth(count, din, dout, s));
     CUDA_TRY(cudaEventRecord(e2, s));
     if (count) CUDA_TRY(cudaMemcpyAsync(linearizations, dout, 23 * sizeof(double) * count, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaEventRecord(e3, s));

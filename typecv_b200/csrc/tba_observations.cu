@@ -164,7 +164,7 @@ void launch_observations(const ObsParams& a, cudaStream_t s) {
 
 // ---- inverse-depth linearisation (linearizeInverseDepth, src/sfm/depth/gpu/inverse-depth.shade.ts) ----
 //
-// One observation per thread.  Input row (34 words): the anchored point's parameters a, b, rho
+// One row per thread.  Input row (34 words): the anchored point's parameters a, b, rho
 // (normalised image coordinates and inverse depth in its reference camera), the reference pose
 // (R row-major, t), the observing pose, the observing camera (fx, fy, cx, cy, k1, k2) and its
 // squared radial limit.  Output row (23 words): valid flag, the projected pixel, the pixel's
@@ -173,16 +173,22 @@ void launch_observations(const ObsParams& a, cudaStream_t s) {
 // q = a A0 + b A1 + A2 + rho T with A_k the observing rotation applied to the reference rotation's
 // k-th row and T the observing rotation applied to the reference centre plus the observing
 // translation: the point scaled by rho, so its projection is unchanged.
+//
+// The rows are 272 and 184 bytes long, so one thread per row reading its own row would touch 32
+// sectors per warp load.  Each block therefore stages its 128 input rows in shared memory with
+// 16-byte loads that are coalesced across the block, computes each row from shared memory, writes
+// the output rows to shared memory and stores them with coalesced 16-byte stores: every DRAM byte
+// is read or written once, in full sectors.  58 KB of shared memory per block leaves three blocks
+// (384 threads, 17 independent 16-byte loads each) resident per SM, enough bytes in flight for HBM.
 namespace tba {
 namespace {
 
-__global__ void __launch_bounds__(256) k_linearize_inverse_depth(uint32_t count, const double* __restrict__ in,
-                                                                  double* __restrict__ out) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const double* m = in + 34 * size_t(i);
-  double* o = out + 23 * size_t(i);
-  for (int k = 0; k < 23; k++) o[k] = 0;
+constexpr int kIdRows = 128;
+constexpr int kIdIn = 34, kIdOut = 23;
+constexpr size_t kIdSmem = size_t(kIdRows) * (kIdIn + kIdOut) * sizeof(double);
+
+__device__ __forceinline__ void inverse_depth_row(const double* m, double* o) {
+  for (int k = 0; k < kIdOut; k++) o[k] = 0;
   const double a = m[0], b = m[1], rho = m[2];
   double cx = 0, cy = 0, cz = 0;
   for (int k = 0; k < 3; k++) {
@@ -230,10 +236,44 @@ __global__ void __launch_bounds__(256) k_linearize_inverse_depth(uint32_t count,
   o[22] = fy * y * d;
 }
 
+// Rows [first, first + n) of this block, n <= kIdRows.  Both arrays start 16-byte aligned (the
+// host checks), and a block's tile starts at a multiple of 128 rows, so the input tile
+// (n * 272 bytes) is whole 16-byte words and the output tile (n * 184 bytes) is whole 16-byte words
+// but for a last 8 bytes when n is odd.
+__global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t count, const double* __restrict__ in,
+                                                                      double* __restrict__ out) {
+  extern __shared__ double4 id_smem4[];
+  double* tile_in = reinterpret_cast<double*>(id_smem4);
+  double* tile_out = tile_in + kIdRows * kIdIn;
+  const uint32_t first = blockIdx.x * kIdRows;
+  const uint32_t n = min(uint32_t(kIdRows), count - first);
+  const double2* src = reinterpret_cast<const double2*>(in + size_t(first) * kIdIn);
+  double2* stage_in = reinterpret_cast<double2*>(tile_in);
+  const uint32_t words_in = n * (kIdIn / 2);
+#pragma unroll 4
+  for (uint32_t w = threadIdx.x; w < words_in; w += kIdRows) stage_in[w] = __ldcs(src + w);
+  __syncthreads();
+  if (threadIdx.x < n) inverse_depth_row(tile_in + threadIdx.x * kIdIn, tile_out + threadIdx.x * kIdOut);
+  __syncthreads();
+  double* dst = out + size_t(first) * kIdOut;
+  const uint32_t doubles_out = n * kIdOut;
+  const uint32_t words_out = doubles_out / 2;
+  const double2* stage_out = reinterpret_cast<const double2*>(tile_out);
+  double2* dst2 = reinterpret_cast<double2*>(dst);
+#pragma unroll 4
+  for (uint32_t w = threadIdx.x; w < words_out; w += kIdRows) __stcs(dst2 + w, stage_out[w]);
+  if ((doubles_out & 1) && threadIdx.x == 0) dst[doubles_out - 1] = tile_out[doubles_out - 1];
+}
+
 }  // namespace
 
-void launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s) {
-  if (count) k_linearize_inverse_depth<<<(count + 255) / 256, 256, 0, s>>>(count, in, out);
+cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_linearize_inverse_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kIdSmem));
+  if (e != cudaSuccess) return e;
+  k_linearize_inverse_depth<<<(count + kIdRows - 1) / kIdRows, kIdRows, kIdSmem, s>>>(count, in, out);
+  return cudaGetLastError();
 }
 
 }  // namespace tba

@@ -24,6 +24,7 @@ struct ObsParams {
 
 void launch_observations(const ObsParams& a, cudaStream_t s);
 // 34 words in, 23 out per observation (tba_observations.cu).
-void launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s);
+// Both arrays 16-byte aligned.
+cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s);
 
 }  // namespace tba
