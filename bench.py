@@ -580,7 +580,7 @@ def run_adjoint(args, world, rank, local):
             "with_outliers": {"observations": sc.M, "gradient_norm_at_lm_solution": rep_out["gradient_norm_initial"],
                               "point_blocks_shifted": rep_out["point_failures"], "failed_bits": rep_out["failed"],
                               "adjoint_residual": rep_out["adjoint_residual"]},
-            "clocks": clk, "gpu_launches": None}
+            "clocks": clk, "gpu_launches": sum(r["kernel_launches"] for r in reps)}
     print(json.dumps(line), flush=True)
 
 

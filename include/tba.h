@@ -306,6 +306,7 @@ typedef struct {
                                    were shifted by the smallest power-of-ten multiple of their mean
                                    diagonal that makes them definite (their derivatives are then
                                    approximate: such points have a nearly flat robust cost) */
+  uint32_t kernel_launches;     /* kernels launched by the call */
 } tba_vjp_report;
 
 tba_status tba_bundle_vjp(tba_device* device, const tba_vjp_control* control, const double* scene, size_t scene_len,

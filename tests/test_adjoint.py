@@ -69,6 +69,8 @@ def test_vjp_matches_the_dense_reference(device):
     g = unit_cotangent(12 * sc.C + 3 * sc.P, 5)
     ybar, kbar, sol, rep = AD.bundle_vjp(device, sc.C, sc.P, sc.M, s, i, g, newton_steps=4, want_solution=True)
     assert rep["failed"] == 0 and rep["adjoint_residual"] < 1e-10
+    # Every PCG step is three launches (point products, camera products, vector update).
+    assert rep["kernel_launches"] >= 3 * rep["cg_iterations"] + 10
     pb = Problem(sc.C, sc.P, sc.M, with_solution(sc, s, sol), i)
     ybar_d, kbar_d = pb.vjp(g)
     assert np.linalg.norm(ybar - ybar_d) <= 1e-6 * np.linalg.norm(ybar_d)

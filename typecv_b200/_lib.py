@@ -97,7 +97,7 @@ class VjpReport(ctypes.Structure):
         ("gradient_norm_initial", ctypes.c_double), ("gradient_norm_final", ctypes.c_double),
         ("adjoint_residual", ctypes.c_double),
         ("cg_iterations", ctypes.c_uint32), ("newton_steps", ctypes.c_uint32), ("failed", ctypes.c_uint32),
-        ("invalid", ctypes.c_uint32), ("point_failures", ctypes.c_uint32),
+        ("invalid", ctypes.c_uint32), ("point_failures", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

@@ -717,46 +717,67 @@ uint32_t grid_for(uint32_t n, uint32_t threads) {
 
 }  // namespace
 
-void adj_launch_init(const AdjParams& a, cudaStream_t s) { k_adj_init<<<1, 1, 0, s>>>(a); }
-void adj_launch_reset(const AdjParams& a, cudaStream_t s) { k_adj_reset<<<1, 32, 0, s>>>(a); }
+// Each launcher returns the number of kernels it launched.
+uint32_t adj_launch_init(const AdjParams& a, cudaStream_t s) {
+  k_adj_init<<<1, 1, 0, s>>>(a);
+  return 1;
+}
+uint32_t adj_launch_reset(const AdjParams& a, cudaStream_t s) {
+  k_adj_reset<<<1, 32, 0, s>>>(a);
+  return 1;
+}
 
-void adj_launch_assemble(const AdjParams& a, cudaStream_t s) {
+uint32_t adj_launch_assemble(const AdjParams& a, cudaStream_t s) {
   k_adj_obs<<<grid_for(a.M, 128), 128, 0, s>>>(a);
   k_adj_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
   k_adj_cameras<<<a.C, 128, 0, s>>>(a);
+  return 3;
 }
 
-void adj_launch_pcg_init(const AdjParams& a, cudaStream_t s) { k_adj_pcg_init<<<1, 1024, 0, s>>>(a); }
+uint32_t adj_launch_pcg_init(const AdjParams& a, cudaStream_t s) {
+  k_adj_pcg_init<<<1, 1024, 0, s>>>(a);
+  return 1;
+}
 
-void adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
+uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
   k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
   k_adj_prod_cameras<<<a.C, 128, 0, s>>>(a);
   k_adj_vec<<<1, 1024, 0, s>>>(a);
+  return 3;
 }
 
-void adj_launch_back_substitute(const AdjParams& a, cudaStream_t s) { k_adj_back<<<grid_for(a.P, 256), 256, 0, s>>>(a); }
+uint32_t adj_launch_back_substitute(const AdjParams& a, cudaStream_t s) {
+  k_adj_back<<<grid_for(a.P, 256), 256, 0, s>>>(a);
+  return 1;
+}
 
-void adj_launch_newton_candidate(const AdjParams& a, cudaStream_t s) {
+uint32_t adj_launch_newton_candidate(const AdjParams& a, cudaStream_t s) {
   k_adj_newton_cameras<<<1, 256, 0, s>>>(a);
   k_adj_newton_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
   k_adj_cost<<<grid_for(a.M, 256), 256, 0, s>>>(a, a.tposes, a.tpoints);
+  return 3;
 }
 
-void adj_launch_newton_commit(const AdjParams& a, cudaStream_t s) {
+uint32_t adj_launch_newton_commit(const AdjParams& a, cudaStream_t s) {
   k_adj_commit<<<grid_for(12 * a.C + 3 * a.P, 256), 256, 0, s>>>(a);
+  return 1;
 }
 
-void adj_launch_cost(const AdjParams& a, cudaStream_t s) {
+uint32_t adj_launch_cost(const AdjParams& a, cudaStream_t s) {
   k_adj_zero_cost<<<1, 1, 0, s>>>(a);
   k_adj_cost<<<grid_for(a.M, 256), 256, 0, s>>>(a, a.poses, a.points);
+  return 2;
 }
 
-void adj_launch_cotangent(const AdjParams& a, const double* cotangent, cudaStream_t s) {
+uint32_t adj_launch_cotangent(const AdjParams& a, const double* cotangent, cudaStream_t s) {
   k_adj_cotangent<<<grid_for(a.C + a.P, 256), 256, 0, s>>>(a, cotangent);
   k_adj_cotangent_project<<<1, 1, 0, s>>>(a);
+  return 2;
 }
 
-void adj_launch_vjp(const AdjParams& a, cudaStream_t s) { k_adj_vjp<<<grid_for(a.M, 128), 128, 0, s>>>(a); }
-
+uint32_t adj_launch_vjp(const AdjParams& a, cudaStream_t s) {
+  k_adj_vjp<<<grid_for(a.M, 128), 128, 0, s>>>(a);
+  return 1;
+}
 
 }  // namespace tba

@@ -79,19 +79,19 @@ struct AdjParams {
   uint32_t rhs_mode;  // 0: Newton (-gradient), 1: adjoint (cot)
 };
 
-void adj_launch_init(const AdjParams& a, cudaStream_t s);        // gauge origin and baseline
-void adj_launch_reset(const AdjParams& a, cudaStream_t s);       // zero the per-solve sums and flags
-void adj_launch_assemble(const AdjParams& a, cudaStream_t s);    // per observation, points, cameras
-void adj_launch_pcg_init(const AdjParams& a, cudaStream_t s);
-void adj_launch_pcg_step(const AdjParams& a, cudaStream_t s);    // product + vector step
-void adj_launch_back_substitute(const AdjParams& a, cudaStream_t s);
+uint32_t adj_launch_init(const AdjParams& a, cudaStream_t s);        // gauge origin and baseline
+uint32_t adj_launch_reset(const AdjParams& a, cudaStream_t s);       // zero the per-solve sums and flags
+uint32_t adj_launch_assemble(const AdjParams& a, cudaStream_t s);    // per observation, points, cameras
+uint32_t adj_launch_pcg_init(const AdjParams& a, cudaStream_t s);
+uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s);    // product + vector step
+uint32_t adj_launch_back_substitute(const AdjParams& a, cudaStream_t s);
 // The candidate theta (+) delta into tposes/tpoints (with the gauge normalisation) and its robust
 // cost into A_COST; then, when accepted, its commit.
-void adj_launch_newton_candidate(const AdjParams& a, cudaStream_t s);
-void adj_launch_newton_commit(const AdjParams& a, cudaStream_t s);
+uint32_t adj_launch_newton_candidate(const AdjParams& a, cudaStream_t s);
+uint32_t adj_launch_newton_commit(const AdjParams& a, cudaStream_t s);
 // The robust cost of the current point into A_COST.
-void adj_launch_cost(const AdjParams& a, cudaStream_t s);
-void adj_launch_cotangent(const AdjParams& a, const double* cotangent, cudaStream_t s);
-void adj_launch_vjp(const AdjParams& a, cudaStream_t s);
+uint32_t adj_launch_cost(const AdjParams& a, cudaStream_t s);
+uint32_t adj_launch_cotangent(const AdjParams& a, const double* cotangent, cudaStream_t s);
+uint32_t adj_launch_vjp(const AdjParams& a, cudaStream_t s);
 
 }  // namespace tba

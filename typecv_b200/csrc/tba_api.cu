@@ -992,7 +992,8 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   up(const_cast<double*>(A.cams), scene + 12 * size_t(C) + 3 * size_t(P), 6 * sizeof(double) * C);
   up(const_cast<double*>(A.pixels), scene + 18 * size_t(C) + 3 * size_t(P), 2 * sizeof(double) * M);
   up(dindex, index, sizeof(uint32_t) * (3 * size_t(M) + P + 2 * size_t(C) + 2));
-  tba::adj_launch_init(A, s);
+  uint32_t launches = 0;
+  launches += tba::adj_launch_init(A, s);
   CUDA_TRY(cudaGetLastError());
 
   auto read_state = [&]() {
@@ -1005,14 +1006,14 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   // and lp (points).  The assembly also measures |F|^2 at the current point.
   auto linear_solve = [&](uint32_t mode, bool cotangent_ready) {
     A.rhs_mode = mode;
-    if (!cotangent_ready) tba::adj_launch_reset(A, s);
-    tba::adj_launch_assemble(A, s);
-    tba::adj_launch_pcg_init(A, s);
+    if (!cotangent_ready) launches += tba::adj_launch_reset(A, s);
+    launches += tba::adj_launch_assemble(A, s);
+    launches += tba::adj_launch_pcg_init(A, s);
     CUDA_TRY(cudaGetLastError());
     uint32_t done = 0;
     while (done < vc->max_cg) {
       const uint32_t k = std::min<uint32_t>(16, vc->max_cg - done);
-      for (uint32_t j = 0; j < k; j++) tba::adj_launch_pcg_step(A, s);
+      for (uint32_t j = 0; j < k; j++) launches += tba::adj_launch_pcg_step(A, s);
       CUDA_TRY(cudaGetLastError());
       done += k;
       read_state();
@@ -1030,7 +1031,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     if (st[tba::A_CAMERA_FAILED] != 0) failed |= 2;
     if (st[tba::A_FAILED] != 0) failed |= 4;
     if (!converged) failed |= 8;
-    tba::adj_launch_back_substitute(A, s);
+    launches += tba::adj_launch_back_substitute(A, s);
     CUDA_TRY(cudaGetLastError());
     return st[tba::A_INVALID];
   };
@@ -1039,7 +1040,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   // robust cost accepts and reaches 0 (exact Newton) below 1e-6, and grows tenfold after a rejected
   // one.  Candidates within a relative 1e-14 of the current cost count as accepted.
   if (vc->newton_steps > 0) {
-    tba::adj_launch_cost(A, s);
+    launches += tba::adj_launch_cost(A, s);
     read_state();
   }
   double cost = d->pinned[tba::A_COST], mu = 1e-2;
@@ -1047,14 +1048,14 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   for (uint32_t k = 0; k < vc->newton_steps; k++) {
     A.mu = mu;
     invalid = linear_solve(0, false);
-    tba::adj_launch_newton_candidate(A, s);
+    launches += tba::adj_launch_newton_candidate(A, s);
     CUDA_TRY(cudaGetLastError());
     read_state();
     const double cand = d->pinned[tba::A_COST];
     const bool solved = (failed & 5) == 0;
     failed &= ~uint32_t(13);  // a damped solve that failed is retried with more damping
     if (solved && cand <= cost * (1 + 1e-14)) {
-      tba::adj_launch_newton_commit(A, s);
+      launches += tba::adj_launch_newton_commit(A, s);
       CUDA_TRY(cudaGetLastError());
       cost = cand;
       accepted++;
@@ -1067,11 +1068,11 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   if (cotangent) {
     double* gcot = D(o_gcot);
     up(gcot, cotangent, sizeof(double) * (12 * size_t(C) + 3 * size_t(P)));
-    tba::adj_launch_reset(A, s);
-    tba::adj_launch_cotangent(A, gcot, s);
+    launches += tba::adj_launch_reset(A, s);
+    launches += tba::adj_launch_cotangent(A, gcot, s);
     CUDA_TRY(cudaGetLastError());
     invalid = linear_solve(1, true);
-    tba::adj_launch_vjp(A, s);
+    launches += tba::adj_launch_vjp(A, s);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(pixels_bar, A.ybar, 2 * sizeof(double) * M, cudaMemcpyDeviceToHost, s));
     read_state();
@@ -1081,9 +1082,9 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     }
   } else if (vc->newton_steps > 0) {
     // The gradient at the final point.
-    tba::adj_launch_reset(A, s);
+    launches += tba::adj_launch_reset(A, s);
     A.rhs_mode = 0;
-    tba::adj_launch_assemble(A, s);
+    launches += tba::adj_launch_assemble(A, s);
     read_state();
     gnorm = std::sqrt(d->pinned[tba::A_GNORM]);
     invalid = d->pinned[tba::A_INVALID];
@@ -1107,6 +1108,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     report->failed = failed;
     report->invalid = uint32_t(invalid);
     report->point_failures = point_failures;
+    report->kernel_launches = launches;
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
   }
 }
