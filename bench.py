@@ -725,18 +725,15 @@ def run_observations(args, world, rank, local):
     wall_s = max_over_ranks(world, sum(walls))
     if rank != 0:
         return
-    # A bounded sample for the oracle: the leading tracks holding about 60k observations.
+    # Every flag against the oracle (the restated kernels in C++, OpenMP over the host cores).
     from oracle import observations as oo
-    h = int(np.searchsorted(req["offsets"], 60000))
-    n = int(req["offsets"][h])
-    sub = {**req, "points": req["points"][:3 * h], "pixels": req["pixels"][:2 * n], "indices": req["indices"][:2 * n],
-           "offsets": req["offsets"][:h + 1], "count": n, "P": h}
+    oo.evaluate_cpp({**req, "count": 64, "P": 1, "offsets": req["offsets"][:2]})
     t0 = time.perf_counter()
-    want = oo.evaluate(sub)
+    want = oo.evaluate_cpp(req)
     cpu_s = time.perf_counter() - t0
-    got_obs = flags[:n]
-    got_tracks = flags[M:M + h]
-    mismatches = int(np.sum(want["flags"][:n] != got_obs) + np.sum(want["flags"][n:n + h] != got_tracks))
+    mismatches = int(np.sum(want["flags"] != flags[:M + P]))
+    summary_rel = abs(want["summary"][0] - summary[0]) / max(abs(want["summary"][0]), 1e-300)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     pk, kind = peaks()
     per_launch_s = kernel_s / args.steps
     algorithmic = 56 * M + 32 * P + 144 * C
@@ -759,10 +756,12 @@ def run_observations(args, world, rank, local):
                          "note": "the whole evaluation (projection, depth filter, partials, summary: "
                                  f"{reps[-1]['kernel_launches']} launches) against 56 B per observation + 32 B per "
                                  f"point + 144 B per camera; peak of {kind}"},
-            "parity": {"observations_checked": n, "tracks_checked": h, "flag_mismatches": mismatches},
-            "cpu_baseline": {"value": n / cpu_s, "unit": "observations/s", "cores": 1, "kind": "port",
-                             "sample": f"the first {h} tracks ({n} observations) through the restated kernels "
-                                       "(oracle/observations.py, pure Python)"},
+            "parity": {"observations_checked": M, "tracks_checked": P, "flag_mismatches": mismatches,
+                       "inlier_count_equal": bool(want["summary"][1] == summary[1]),
+                       "error_sum_rel_diff": summary_rel},
+            "cpu_baseline": {"value": M / cpu_s, "unit": "observations/s", "cores": threads, "kind": "port",
+                             "sample": "every observation of the scene through the restated kernels in C++ "
+                                       "(oracle/ba_oracle.cpp, OpenMP)"},
             "clocks": clocks.summary(), "gpu_launches": sum(r["kernel_launches"] for r in reps)}
     print(json.dumps(line), flush=True)
 

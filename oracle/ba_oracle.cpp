@@ -20,6 +20,11 @@
 //      src/geometry/camera.ts:15-61) over rows in the device's 34-word layout, written in the
 //      device's 23-word layout: the checker and CPU baseline of the inverse-depth linearisation.
 //
+//  (4) `oracle_evaluate_observations`: the observation-evaluation kernels
+//      (src/geometry/gpu/observation-evaluation.shade.ts: projection and threshold, the per-track
+//      depth-sensitivity filter, per-64 partials and their sum) over the packed request, as
+//      oracle/observations.py restates them in Python: the CPU baseline of that evaluation.
+//
 // All are compiled with -ffp-contract=off and no FMA so that every product and sum rounds the
 // way the reference's JavaScript does.  Parity is pinned by tests/golden (see tests/).  The
 // operator's per-point, per-observation and per-camera-row loops run under OpenMP: their
@@ -1538,6 +1543,135 @@ extern "C" {
 void oracle_linearize_inverse_depth(uint32_t n, const double* in, double* out) {
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < int64_t(n); i++) inverse_depth_row(in + 34 * i, out + 23 * i);
+}
+
+}  // extern "C"
+
+// =================================================================================================
+// (4) Observation evaluation (projectIndexedObservations, filterIndexedObservationDepth,
+//     indexedObservationPartials, observationSummary), independent loops under OpenMP.
+namespace {
+
+struct ObsRecord {
+  Pose pose;
+  Camera k;
+};
+
+ObsRecord obs_record(const double* cameras, const uint32_t* indices, int64_t i) {
+  const double* r = cameras + 18 * size_t(indices[2 * i]);
+  ObsRecord out;
+  for (int j = 0; j < 9; j++) out.pose.R[j] = r[j];
+  for (int j = 0; j < 3; j++) out.pose.t[j] = r[9 + j];
+  out.k = Camera{r[12], r[13], r[14], r[15], r[16], r[17]};
+  return out;
+}
+
+void obs_transform(const Pose& p, const double* X, double q[3]) {
+  for (int r = 0; r < 3; r++) q[r] = p.R[3 * r] * X[0] + p.R[3 * r + 1] * X[1] + p.R[3 * r + 2] * X[2] + p.t[r];
+}
+
+bool obs_stable_depth(const double* cameras, const uint32_t* indices, const uint32_t* flags, uint32_t start,
+                      uint32_t end, const double* X, double noise, double limit) {
+  double A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t count = 0;
+  for (uint32_t i = start; i < end; i++) {
+    if (flags[i] == 0) continue;
+    count++;
+    const ObsRecord rec = obs_record(cameras, indices, i);
+    double q[3];
+    obs_transform(rec.pose, X, q);
+    const Projection pr = op_project(rec.k, q);
+    if (!pr.ok) return false;
+    for (int row = 0; row < 2; row++) {
+      const double* g = row == 0 ? pr.du : pr.dv;
+      const double* R = rec.pose.R;
+      const double J[3] = {g[0] * R[0] + g[1] * R[3] + g[2] * R[6], g[0] * R[1] + g[1] * R[4] + g[2] * R[7],
+                           g[0] * R[2] + g[1] * R[5] + g[2] * R[8]};
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) A[3 * r + c] += J[r] * J[c];
+    }
+  }
+  if (count < 2) return false;
+  for (uint32_t i = start; i < end; i++) {
+    if (flags[i] == 0) continue;
+    const ObsRecord rec = obs_record(cameras, indices, i);
+    const double axis[3] = {rec.pose.R[6], rec.pose.R[7], rec.pose.R[8]};
+    double q[3], s[3];
+    obs_transform(rec.pose, X, q);
+    if (!op_solve3(A, axis, s) || !(q[2] > 0)) return false;
+    const double variance = axis[0] * s[0] + axis[1] * s[1] + axis[2] * s[2];
+    if (!(variance >= 0)) return false;
+    if (!(noise * std::sqrt(variance) / q[2] <= limit)) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The packed request of tba_evaluate_observations: 18-word camera records, 3 words per point, 2 per
+// pixel, (camera, point) per observation, P + 1 track offsets.  flags: M observation flags, then P
+// track flags when guarded; errors: M; summary: inlier error sum, inlier count.
+void oracle_evaluate_observations(uint32_t P, uint32_t M, uint32_t guarded, double max_error, double noise,
+                                  double limit, const double* cameras, const double* points, const double* pixels,
+                                  const uint32_t* indices, const uint32_t* offsets, uint32_t* flags, double* errors,
+                                  double* summary) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < int64_t(M); i++) {
+    flags[i] = 0;
+    errors[i] = 0;
+    const ObsRecord rec = obs_record(cameras, indices, i);
+    double q[3];
+    obs_transform(rec.pose, points + 3 * size_t(indices[2 * i + 1]), q);
+    const Projection pr = op_project(rec.k, q);
+    if (!pr.ok) continue;
+    const double x = pr.pixel[0] - pixels[2 * i], y = pr.pixel[1] - pixels[2 * i + 1];
+    const double e = std::sqrt(x * x + y * y);
+    if (e <= max_error) {
+      flags[i] = 1;
+      errors[i] = e;
+    }
+  }
+  if (guarded) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t h = 0; h < int64_t(P); h++) {
+      const uint32_t start = offsets[h], end = offsets[h + 1];
+      flags[M + h] = 0;
+      if (end <= start) continue;
+      uint32_t accepted = 0;
+      for (uint32_t i = start; i < end; i++) accepted += flags[i] != 0;
+      if (accepted < 2) continue;
+      const double* X = points + 3 * size_t(indices[2 * size_t(start) + 1]);
+      if (!obs_stable_depth(cameras, indices, flags, start, end, X, noise, limit)) {
+        flags[M + h] = 1;
+        for (uint32_t i = start; i < end; i++) {
+          flags[i] = 0;
+          errors[i] = 0;
+        }
+      }
+    }
+  }
+  const int64_t runs = (int64_t(M) + 63) / 64;
+  std::vector<double> pe(runs), pn(runs);
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < runs; b++) {
+    double e = 0, n = 0;
+    for (int64_t i = 64 * b; i < std::min<int64_t>(M, 64 * b + 64); i++)
+      if (flags[i]) {
+        e += errors[i];
+        n += 1;
+      }
+    pe[b] = e;
+    pn[b] = n;
+  }
+  double te = 0, tn = 0;
+  for (int64_t b = 0; b < runs; b++) {
+    te += pe[b];
+    tn += pn[b];
+  }
+  summary[0] = te;
+  summary[1] = tn;
 }
 
 }  // extern "C"

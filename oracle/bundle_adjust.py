@@ -72,6 +72,12 @@ def lib():
                                              P(ctypes.c_double)]
         _lib.oracle_linearize_inverse_depth.restype = None
         _lib.oracle_linearize_inverse_depth.argtypes = [ctypes.c_uint32, P(ctypes.c_double), P(ctypes.c_double)]
+        _lib.oracle_evaluate_observations.restype = None
+        _lib.oracle_evaluate_observations.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
+                                                      ctypes.c_double, ctypes.c_double, P(ctypes.c_double),
+                                                      P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_uint32),
+                                                      P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_double),
+                                                      P(ctypes.c_double)]
         _lib.oracle_metrics.restype = None
         _lib.oracle_metrics.argtypes = [P(Control), P(ctypes.c_double), P(ctypes.c_uint32), P(ctypes.c_double)]
     return _lib

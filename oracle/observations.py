@@ -163,3 +163,21 @@ def evaluate(req) -> dict:
         total_e += e
         total_n += n
     return {"flags": flags, "errors": errors, "summary": np.array([total_e, total_n])}
+
+
+def evaluate_cpp(req) -> dict:
+    """The same evaluation by the C++ restatement (oracle/ba_oracle.cpp, OpenMP over the host cores)."""
+    from oracle import bundle_adjust as ob
+    M, P = req["count"], req["P"]
+    flags = np.zeros(max(1, M + (P if req["guarded"] else 0)), dtype=np.uint32)
+    errors = np.zeros(max(1, M))
+    summary = np.zeros(2)
+    arr = {k: np.ascontiguousarray(req[k]) for k in ("cameras", "points", "pixels")}
+    idx = np.ascontiguousarray(req["indices"], dtype=np.uint32)
+    off = np.ascontiguousarray(req["offsets"], dtype=np.uint32)
+    ob.lib().oracle_evaluate_observations(P, M, 1 if req["guarded"] else 0, float(req["max_error"]),
+                                          float(req["noise"]), float(req["limit"]), ob._dptr(arr["cameras"]),
+                                          ob._dptr(arr["points"]), ob._dptr(arr["pixels"]), ob._uptr(idx),
+                                          ob._uptr(off), ob._uptr(flags), ob._dptr(errors), ob._dptr(summary))
+    return {"flags": flags[:M + (P if req["guarded"] else 0)], "errors": errors[:M], "summary": summary}
+

@@ -164,3 +164,17 @@ def test_cuda_evaluation_of_a_solved_scene_and_its_last_observations():
         want = oracle_result(scene, None, 3.0, last_only=True)
         assert last["inlierCount"] == want["inlierCount"]
         assert all(len(m) == 1 for m in last["masks"])
+
+
+def test_cpp_restatement_matches_the_python_one():
+    """oracle_evaluate_observations (ba_oracle.cpp) against oracle/observations.py: identical flags,
+    errors and summary on a guarded and an unguarded request of a synthetic scene with outliers."""
+    import bench
+    from oracle import observations as oo
+    sc = bench.make_scene("cfg2", 0.01)
+    for limit in (0.05, 0.0):
+        req = bench.observation_request(sc, limit=limit)
+        a, b = oo.evaluate(req), oo.evaluate_cpp(req)
+        assert np.array_equal(a["flags"], b["flags"]) and np.array_equal(a["errors"], b["errors"])
+        assert np.array_equal(a["summary"], b["summary"])
+        assert 0 < a["summary"][1] < req["count"]
