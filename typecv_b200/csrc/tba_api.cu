@@ -1582,6 +1582,7 @@ tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const doub
     const auto wall0 = std::chrono::steady_clock::now();
     Layout L;
     const size_t o_in = L.take<double>(34 * size_t(count)), o_out = L.take<double>(23 * size_t(count));
+    const size_t o_err = L.take<uint32_t>(1);
     if (d->capacity < L.bytes) {
       if (d->arena) CUDA_TRY(cudaFree(d->arena));
       d->arena = nullptr;
@@ -1594,16 +1595,21 @@ tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const doub
     }
     double* din = reinterpret_cast<double*>(d->arena + o_in);
     double* dout = reinterpret_cast<double*>(d->arena + o_out);
+    uint32_t* derr = reinterpret_cast<uint32_t*>(d->arena + o_err);
+    uint32_t err = 0;
     cudaStream_t s = d->stream;
     cudaEvent_t e0 = event(d, 0), e1 = event(d, 1), e2 = event(d, 2), e3 = event(d, 3);
+    CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(uint32_t), s));
     CUDA_TRY(cudaEventRecord(e0, s));
     if (count) CUDA_TRY(cudaMemcpyAsync(din, measurements, 34 * sizeof(double) * count, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaEventRecord(e1, s));
-    CUDA_TRY(tba::launch_linearize_inverse_depth(count, din, dout, s));
+    CUDA_TRY(tba::launch_linearize_inverse_depth(count, din, dout, derr, d->sms, s));
     CUDA_TRY(cudaEventRecord(e2, s));
     if (count) CUDA_TRY(cudaMemcpyAsync(linearizations, dout, 23 * sizeof(double) * count, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaEventRecord(e3, s));
+    CUDA_TRY(cudaMemcpyAsync(&err, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) throw Fail{TBA_ERROR_CUDA, "Inverse-depth linearization: a tile load did not complete"};
     if (report) {
       std::memset(report, 0, sizeof *report);
       float ms = 0;

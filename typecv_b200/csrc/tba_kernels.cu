@@ -626,20 +626,42 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
   double ef = 0;
   uint32_t tb, te;
   block_tasks(P, tb, te);
-  uint32_t t = tb + warp;
-  uint32_t o_next = t < te ? P.task_obs[t] : 0, e_next = t < te ? P.task_obs[t + 1] : 0;
-  for (; t < te; t += nwarps) {
-    const uint32_t o0 = o_next, n = e_next - o0;
-    if (t + nwarps < te) {  // the next task's bounds, early
-      o_next = P.task_obs[t + nwarps];
-      e_next = P.task_obs[t + nwarps + 1];
+  // Software pipeline over the warp's tasks: the bounds of a task are loaded two tasks ahead of
+  // its turn and its lane's camera and point index one task ahead, so that when a task's turn
+  // comes its factors, its point's V_p^-1 and its camera's direction are all issued at once and
+  // the task waits for one memory latency instead of two (index, then point block).
+  auto bounds = [&](uint32_t tt, uint32_t& o, uint32_t& e) {
+    o = e = 0;
+    if (tt < te) {
+      o = P.task_obs[tt];
+      e = P.task_obs[tt + 1];
     }
+  };
+  auto lane_indices = [&](uint32_t o, uint32_t e, uint32_t& c, uint32_t& pt) {
+    c = pt = 0;
+    const uint32_t n = e - o;
+    if (n == 0 || n > uint32_t(kTaskObs)) return;
+    const uint32_t i = o + min(uint32_t(lane), n - 1);
+    c = P.obs_camera[i];
+    pt = P.obs_point[i];
+  };
+  uint32_t t = tb + warp;
+  uint32_t o_cur, e_cur, o_nx, e_nx, c_cur, pt_cur;
+  bounds(t, o_cur, e_cur);
+  bounds(t + nwarps, o_nx, e_nx);
+  lane_indices(o_cur, e_cur, c_cur, pt_cur);
+  for (; t < te; t += nwarps) {
+    const uint32_t o0 = o_cur, n = e_cur - o0;
+    const uint32_t c = c_cur, pt = pt_cur;
+    o_cur = o_nx;
+    e_cur = e_nx;
+    bounds(t + 2 * nwarps, o_nx, e_nx);
+    lane_indices(o_cur, e_cur, c_cur, pt_cur);
     if (n <= uint32_t(kTaskObs)) {
       // One observation per lane.  Every load the lane needs is issued before any arithmetic: its
-      // camera and point index, its factors, its point's V_p^-1 and its camera's direction.
+      // factors, its point's V_p^-1 and its camera's direction (its indices came a task earlier).
       const bool valid = uint32_t(lane) < n;
       const uint32_t i = o0 + (valid ? lane : 0);
-      const uint32_t c = P.obs_camera[i], pt = P.obs_point[i];
       Factors<T> f;
       load_factors(FT, stride, i, f);
       double vb[6], xw[6];

@@ -18,6 +18,8 @@
 // observation pixel, and per observation its camera and point index interleaved.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "tba_math.cuh"
 #include "tba_observations.cuh"
 
@@ -174,18 +176,53 @@ void launch_observations(const ObsParams& a, cudaStream_t s) {
 // k-th row and T the observing rotation applied to the reference centre plus the observing
 // translation: the point scaled by rho, so its projection is unchanged.
 //
-// The rows are 272 and 184 bytes long, so one thread per row reading its own row would touch 32
-// sectors per warp load.  Each block therefore stages its 128 input rows in shared memory with
-// 16-byte loads that are coalesced across the block, computes each row from shared memory, writes
-// the output rows to shared memory and stores them with coalesced 16-byte stores: every DRAM byte
-// is read or written once, in full sectors.  58 KB of shared memory per block leaves three blocks
-// (384 threads, 17 independent 16-byte loads each) resident per SM, enough bytes in flight for HBM.
+// The rows are 272 and 184 bytes long, so one thread per row reading its own row from global
+// memory would touch 32 sectors per warp load.  Instead the kernel is persistent (two blocks per
+// SM) and streams tiles of 128 rows through shared memory with the bulk-copy engine: the block's
+// producer thread keeps two input tiles in flight (cp.async.bulk global -> shared, completion on
+// an mbarrier per stage), the 128 threads compute one row each from shared memory into an output
+// tile, and the producer writes the output tile back with one bulk store (cp.async.bulk
+// shared -> global).  Every DRAM byte moves once, in whole lines, with no register cost for the
+// bytes in flight (two blocks x two 34.8 KB tiles per SM).  Waits on an mbarrier are bounded: a
+// wait that runs out sets the error word and the block stops.
 namespace tba {
 namespace {
 
 constexpr int kIdRows = 128;
 constexpr int kIdIn = 34, kIdOut = 23;
-constexpr size_t kIdSmem = size_t(kIdRows) * (kIdIn + kIdOut) * sizeof(double);
+constexpr int kIdStages = 2;
+constexpr uint32_t kIdTileIn = kIdRows * kIdIn * 8, kIdTileOut = kIdRows * kIdOut * 8;
+constexpr size_t kIdSmem = size_t(kIdStages) * kIdTileIn + kIdTileOut + 64;
+constexpr uint32_t kIdWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void id_bar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+
+// One arrival that also announces `bytes` of transactions, then the bulk load that completes them.
+__device__ __forceinline__ void id_load_tile(uint32_t bar, uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool id_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t k = 0; k < kIdWaitLimit; k++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 __device__ __forceinline__ void inverse_depth_row(const double* m, double* o) {
   for (int k = 0; k < kIdOut; k++) o[k] = 0;
@@ -236,43 +273,77 @@ __device__ __forceinline__ void inverse_depth_row(const double* m, double* o) {
   o[22] = fy * y * d;
 }
 
-// Rows [first, first + n) of this block, n <= kIdRows.  Both arrays start 16-byte aligned (the
-// host checks), and a block's tile starts at a multiple of 128 rows, so the input tile
-// (n * 272 bytes) is whole 16-byte words and the output tile (n * 184 bytes) is whole 16-byte words
-// but for a last 8 bytes when n is odd.
+// Tiles of kIdRows rows; tile k starts at row k * kIdRows, so both tiles' global addresses are
+// 16-byte aligned when the arrays are, and an input tile (n * 272 bytes) is whole 16-byte words.
+// An output tile (n * 184 bytes) is whole 16-byte words but for a last 8 bytes when n is odd; those
+// are written with a plain store.
 __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t count, const double* __restrict__ in,
-                                                                      double* __restrict__ out) {
-  extern __shared__ double4 id_smem4[];
-  double* tile_in = reinterpret_cast<double*>(id_smem4);
-  double* tile_out = tile_in + kIdRows * kIdIn;
-  const uint32_t first = blockIdx.x * kIdRows;
-  const uint32_t n = min(uint32_t(kIdRows), count - first);
-  const double2* src = reinterpret_cast<const double2*>(in + size_t(first) * kIdIn);
-  double2* stage_in = reinterpret_cast<double2*>(tile_in);
-  const uint32_t words_in = n * (kIdIn / 2);
-#pragma unroll 4
-  for (uint32_t w = threadIdx.x; w < words_in; w += kIdRows) stage_in[w] = __ldcs(src + w);
+                                                                      double* __restrict__ out, uint32_t* error) {
+  extern __shared__ __align__(128) unsigned char id_smem[];
+  double* stage = reinterpret_cast<double*>(id_smem);
+  double* tile_out = reinterpret_cast<double*>(id_smem + kIdStages * size_t(kIdTileIn));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(id_smem + kIdStages * size_t(kIdTileIn) + kIdTileOut);
+  __shared__ uint32_t abort_flag;
+  const uint32_t tiles = (count + kIdRows - 1) / kIdRows;
+  const bool producer = threadIdx.x == 0;
+  auto rows_of = [&](uint32_t tile) { return min(uint32_t(kIdRows), count - tile * kIdRows); };
+  if (producer) {
+    abort_flag = 0;
+    for (int k = 0; k < kIdStages; k++) id_bar_init(smem_addr(bars + k));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int k = 0; k < kIdStages; k++) {
+      const uint32_t tile = blockIdx.x + k * gridDim.x;
+      if (tile < tiles)
+        id_load_tile(smem_addr(bars + k), smem_addr(stage + size_t(k) * kIdRows * kIdIn),
+                     in + size_t(tile) * kIdRows * kIdIn, rows_of(tile) * kIdIn * 8);
+    }
+  }
   __syncthreads();
-  if (threadIdx.x < n) inverse_depth_row(tile_in + threadIdx.x * kIdIn, tile_out + threadIdx.x * kIdOut);
-  __syncthreads();
-  double* dst = out + size_t(first) * kIdOut;
-  const uint32_t doubles_out = n * kIdOut;
-  const uint32_t words_out = doubles_out / 2;
-  const double2* stage_out = reinterpret_cast<const double2*>(tile_out);
-  double2* dst2 = reinterpret_cast<double2*>(dst);
-#pragma unroll 4
-  for (uint32_t w = threadIdx.x; w < words_out; w += kIdRows) __stcs(dst2 + w, stage_out[w]);
-  if ((doubles_out & 1) && threadIdx.x == 0) dst[doubles_out - 1] = tile_out[doubles_out - 1];
+  uint32_t k = 0;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, k++) {
+    const uint32_t s = k % kIdStages, parity = (k / kIdStages) & 1;
+    const uint32_t n = rows_of(tile);
+    if (!id_wait(smem_addr(bars + s), parity)) {
+      atomicExch(error, 1u);
+      abort_flag = 1;
+    }
+    // The previous tile's bulk store has to have read the output tile before it is rewritten.
+    if (producer) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    __syncthreads();
+    if (abort_flag) break;
+    double* rows = stage + size_t(s) * kIdRows * kIdIn;
+    if (threadIdx.x < n) inverse_depth_row(rows + threadIdx.x * kIdIn, tile_out + threadIdx.x * kIdOut);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (producer) {
+      double* dst = out + size_t(tile) * kIdRows * kIdOut;
+      const uint32_t bytes = n * kIdOut * 8, whole = bytes & ~15u;
+      asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(tile_out)),
+                   "r"(whole)
+                   : "memory");
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      if (whole != bytes) dst[n * kIdOut - 1] = tile_out[n * kIdOut - 1];
+      // Refill this stage with the tile kIdStages turns ahead: every thread has finished reading it.
+      const uint32_t next = tile + kIdStages * gridDim.x;
+      if (next < tiles)
+        id_load_tile(smem_addr(bars + s), smem_addr(rows), in + size_t(next) * kIdRows * kIdIn,
+                     rows_of(next) * kIdIn * 8);
+    }
+  }
+  if (producer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 }  // namespace
 
-cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s) {
+cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, uint32_t* error,
+                                           int sms, cudaStream_t s) {
   if (!count) return cudaSuccess;
   const cudaError_t e =
       cudaFuncSetAttribute(k_linearize_inverse_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kIdSmem));
   if (e != cudaSuccess) return e;
-  k_linearize_inverse_depth<<<(count + kIdRows - 1) / kIdRows, kIdRows, kIdSmem, s>>>(count, in, out);
+  const uint32_t tiles = (count + kIdRows - 1) / kIdRows;
+  const uint32_t grid = std::min<uint32_t>(tiles, 2u * uint32_t(sms > 0 ? sms : 1));
+  k_linearize_inverse_depth<<<grid, kIdRows, kIdSmem, s>>>(count, in, out, error);
   return cudaGetLastError();
 }
 

@@ -24,7 +24,8 @@ struct ObsParams {
 
 void launch_observations(const ObsParams& a, cudaStream_t s);
 // 34 words in, 23 out per observation (tba_observations.cu).
-// Both arrays 16-byte aligned.
-cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, cudaStream_t s);
+// Both arrays 16-byte aligned; *error (zeroed by the caller) becomes 1 if a tile's load never completed.
+cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, uint32_t* error,
+                                           int sms, cudaStream_t s);
 
 }  // namespace tba
