@@ -1389,7 +1389,8 @@ tba_status tba_evaluate_observations(tba_device* d, const tba_observation_contro
           oc->max_relative_depth_std <= 1e9) ||
         !(std::isfinite(oc->pixel_noise_std_px) && oc->pixel_noise_std_px > 0 && oc->pixel_noise_std_px <= 1e9))
       argument("Invalid GPU observation threshold");
-    if (2 * M + P + 1 > 0xffffffffull || 18 * C > 0xffffffffull) argument("GPU observation evaluation exceeds budget");
+    if (2 * M + P + 1 > 0xffffffffull || 18 * C > 0xffffffffull || 8 * P > 0xffffffffull)
+      argument("GPU observation evaluation exceeds budget");
     if ((C && !cameras) || (P && !points) || (M && (!pixels || !indices)) || ((M || guarded) && !flags))
       argument("Invalid GPU observation arrays: null pointer");
     if (cameras_len < 18 * C || points_len < 3 * P || pixels_len < 2 * M || indices_len < 2 * M ||

@@ -609,6 +609,10 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // STAGED: the direction of every camera (world axes, 6C values of T) is staged in shared memory
 // after the camera sums, so the per-observation read of it is an on-chip gather; one block of
 // kStagedThreads per SM.  Otherwise it is read from global memory, two blocks of kProductThreads.
+// Both shared arrays are component-major (value j of camera c at j * C + c): the lanes of a warp
+// touch random cameras, and with camera-major records of 6 words the 8-byte accesses of a warp
+// would fall on only 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over
+// all 16.
 template <bool SHARED, typename T, bool STAGED>
 __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double acc[];
@@ -616,8 +620,9 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
   const uint32_t m = P.m;
   T* pws = reinterpret_cast<T*>(acc + ((m + 1) & ~1u));
   for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) acc[j] = 0;
+  const uint32_t C = P.C;
   if (STAGED)
-    for (uint32_t j = threadIdx.x; j < 6 * P.C; j += blockDim.x) pws[j] = T(P.pw[j]);
+    for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) pws[(j % 6) * C + j / 6] = T(P.pw[j]);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const T* FT = sizeof(T) == 4 ? reinterpret_cast<const T*>(P.F32) : reinterpret_cast<const T*>(P.F);
@@ -626,48 +631,26 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
   double ef = 0;
   uint32_t tb, te;
   block_tasks(P, tb, te);
-  // Software pipeline over the warp's tasks: the bounds of a task are loaded two tasks ahead of
-  // its turn and its lane's camera and point index one task ahead, so that when a task's turn
-  // comes its factors, its point's V_p^-1 and its camera's direction are all issued at once and
-  // the task waits for one memory latency instead of two (index, then point block).
-  auto bounds = [&](uint32_t tt, uint32_t& o, uint32_t& e) {
-    o = e = 0;
-    if (tt < te) {
-      o = P.task_obs[tt];
-      e = P.task_obs[tt + 1];
-    }
-  };
-  auto lane_indices = [&](uint32_t o, uint32_t e, uint32_t& c, uint32_t& pt) {
-    c = pt = 0;
-    const uint32_t n = e - o;
-    if (n == 0 || n > uint32_t(kTaskObs)) return;
-    const uint32_t i = o + min(uint32_t(lane), n - 1);
-    c = P.obs_camera[i];
-    pt = P.obs_point[i];
-  };
   uint32_t t = tb + warp;
-  uint32_t o_cur, e_cur, o_nx, e_nx, c_cur, pt_cur;
-  bounds(t, o_cur, e_cur);
-  bounds(t + nwarps, o_nx, e_nx);
-  lane_indices(o_cur, e_cur, c_cur, pt_cur);
+  uint32_t o_next = t < te ? P.task_obs[t] : 0, e_next = t < te ? P.task_obs[t + 1] : 0;
   for (; t < te; t += nwarps) {
-    const uint32_t o0 = o_cur, n = e_cur - o0;
-    const uint32_t c = c_cur, pt = pt_cur;
-    o_cur = o_nx;
-    e_cur = e_nx;
-    bounds(t + 2 * nwarps, o_nx, e_nx);
-    lane_indices(o_cur, e_cur, c_cur, pt_cur);
+    const uint32_t o0 = o_next, n = e_next - o0;
+    if (t + nwarps < te) {  // the next task's bounds, early
+      o_next = P.task_obs[t + nwarps];
+      e_next = P.task_obs[t + nwarps + 1];
+    }
     if (n <= uint32_t(kTaskObs)) {
       // One observation per lane.  Every load the lane needs is issued before any arithmetic: its
-      // factors, its point's V_p^-1 and its camera's direction (its indices came a task earlier).
+      // camera and point index, its factors, its point's V_p^-1 and its camera's direction.
       const bool valid = uint32_t(lane) < n;
       const uint32_t i = o0 + (valid ? lane : 0);
+      const uint32_t c = P.obs_camera[i], pt = P.obs_point[i];
       Factors<T> f;
       load_factors(FT, stride, i, f);
       double vb[6], xw[6];
       load6(P.pblk + 12 * size_t(pt), vb);
       if (STAGED)
-        for (int j = 0; j < 6; j++) xw[j] = double(pws[6 * c + j]);
+        for (int j = 0; j < 6; j++) xw[j] = double(pws[j * C + c]);
       else
         load6(P.pw + 6 * size_t(c), xw);
       // A fixed camera's direction is zero, so its observations add nothing on the camera side;
@@ -694,14 +677,14 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      double* ac = acc + 6 * size_t(c);
-      atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + 1, -double(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2, -double(f.q[0] * h1 - f.q[1] * h0));
+      double* ac = acc + c;
+      atomicAdd(ac, -double(f.q[1] * h2 - f.q[2] * h1));
+      atomicAdd(ac + C, -double(f.q[2] * h0 - f.q[0] * h2));
+      atomicAdd(ac + 2 * C, -double(f.q[0] * h1 - f.q[1] * h0));
       if (!directional(P, pt)) {
-        atomicAdd(ac + 3, -double(h0));
-        atomicAdd(ac + 4, -double(h1));
-        atomicAdd(ac + 5, -double(h2));
+        atomicAdd(ac + 3 * C, -double(h0));
+        atomicAdd(ac + 4 * C, -double(h1));
+        atomicAdd(ac + 5 * C, -double(h2));
       }
       continue;
     }
@@ -718,7 +701,7 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
         load_factors(FT, stride, i, f);
         double xw[6], u[3];
         if (STAGED)
-          for (int j = 0; j < 6; j++) xw[j] = double(pws[6 * c + j]);
+          for (int j = 0; j < 6; j++) xw[j] = double(pws[j * C + c]);
         else
           load6(P.pw + 6 * size_t(c), xw);
         factor_wt(f, xw, pf, true, directional(P, p0), SHARED, u);
@@ -744,14 +727,14 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      double* ac = acc + 6 * size_t(c);
-      atomicAdd(ac + 0, -double(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + 1, -double(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2, -double(f.q[0] * h1 - f.q[1] * h0));
+      double* ac = acc + c;
+      atomicAdd(ac, -double(f.q[1] * h2 - f.q[2] * h1));
+      atomicAdd(ac + C, -double(f.q[2] * h0 - f.q[0] * h2));
+      atomicAdd(ac + 2 * C, -double(f.q[0] * h1 - f.q[1] * h0));
       if (!directional(P, p0)) {
-        atomicAdd(ac + 3, -double(h0));
-        atomicAdd(ac + 4, -double(h1));
-        atomicAdd(ac + 5, -double(h2));
+        atomicAdd(ac + 3 * C, -double(h0));
+        atomicAdd(ac + 4 * C, -double(h1));
+        atomicAdd(ac + 5 * C, -double(h2));
       }
     }
   }
@@ -762,8 +745,9 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
   __syncthreads();
   // Rotate each camera's sums into its axes and write this block's partial row.
   double* out = P.acc_part + size_t(blockIdx.x) * m;
-  for (uint32_t c = threadIdx.x; c < P.C; c += blockDim.x) {
-    const double* a = acc + 6 * size_t(c);
+  for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
+    double a[6];
+    for (int j = 0; j < 6; j++) a[j] = acc[j * C + c];
     const double* R = P.poses + 12 * size_t(c);
     for (int r = 0; r < 3; r++) {
       out[6 * c + r] = R[3 * r] * a[0] + R[3 * r + 1] * a[1] + R[3 * r + 2] * a[2];
