@@ -32,6 +32,8 @@
 // shared-memory camera sums of k_product_f, whose FP64 atomic adds commute only up to rounding.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "tba_engine.cuh"
 #include "tba_warp.cuh"
 
@@ -609,20 +611,25 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // STAGED: the direction of every camera (world axes, 6C values of T) is staged in shared memory
 // after the camera sums, so the per-observation read of it is an on-chip gather; one block of
 // kStagedThreads per SM.  Otherwise it is read from global memory, two blocks of kProductThreads.
-// Both shared arrays are component-major (value j of camera c at j * C + c): the lanes of a warp
-// touch random cameras, and with camera-major records of 6 words the 8-byte accesses of a warp
-// would fall on only 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over
-// all 16.
+// Both shared arrays are component-major (the sums: value j of camera c at j * C + c; the direction:
+// pair k of camera c at k * C + c, read as one 16- or 8-byte word): the lanes of a warp touch random
+// cameras, and with camera-major records of 6 words the 8-byte accesses of a warp would fall on only
+// 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over all of them.
 template <bool SHARED, typename T, bool STAGED>
 __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double acc[];
   if (P.state[S_CG_ACTIVE] == 0) return;
   const uint32_t m = P.m;
-  T* pws = reinterpret_cast<T*>(acc + ((m + 1) & ~1u));
+  // The staged direction: three arrays of C pairs (pair k of each camera's 6 values).
+  using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  T2* pws = reinterpret_cast<T2*>(acc + ((m + 1) & ~1u));
   for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) acc[j] = 0;
   const uint32_t C = P.C;
   if (STAGED)
-    for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) pws[(j % 6) * C + j / 6] = T(P.pw[j]);
+    for (uint32_t j = threadIdx.x; j < 3 * C; j += blockDim.x) {
+      const uint32_t c = j / 3, k = j % 3;
+      pws[k * C + c] = T2{T(P.pw[6 * c + 2 * k]), T(P.pw[6 * c + 2 * k + 1])};
+    }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const T* FT = sizeof(T) == 4 ? reinterpret_cast<const T*>(P.F32) : reinterpret_cast<const T*>(P.F);
@@ -650,7 +657,11 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
       double vb[6], xw[6];
       load6(P.pblk + 12 * size_t(pt), vb);
       if (STAGED)
-        for (int j = 0; j < 6; j++) xw[j] = double(pws[j * C + c]);
+        for (int k = 0; k < 3; k++) {
+          const T2 v = pws[k * C + c];
+          xw[2 * k] = double(v.x);
+          xw[2 * k + 1] = double(v.y);
+        }
       else
         load6(P.pw + 6 * size_t(c), xw);
       // A fixed camera's direction is zero, so its observations add nothing on the camera side;
@@ -701,7 +712,11 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
         load_factors(FT, stride, i, f);
         double xw[6], u[3];
         if (STAGED)
-          for (int j = 0; j < 6; j++) xw[j] = double(pws[j * C + c]);
+          for (int k = 0; k < 3; k++) {
+            const T2 v = pws[k * C + c];
+            xw[2 * k] = double(v.x);
+            xw[2 * k + 1] = double(v.y);
+          }
         else
           load6(P.pw + 6 * size_t(c), xw);
         factor_wt(f, xw, pf, true, directional(P, p0), SHARED, u);
