@@ -617,14 +617,17 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over all of them.
 template <bool SHARED, typename T, bool STAGED>
 __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STAGED ? 1 : 2) k_product_f(Params P) {
-  extern __shared__ double acc[];
+  extern __shared__ double4 product_smem[];
+  __shared__ double focal_acc;
   if (P.state[S_CG_ACTIVE] == 0) return;
-  const uint32_t m = P.m;
-  // The staged direction: three arrays of C pairs (pair k of each camera's 6 values).
+  const uint32_t m = P.m, C = P.C;
+  // The camera sums (6C values of T: FP64 sums for FP64 factors, FP32 sums of a block's share for
+  // FP32 factors), then the staged direction: three arrays of C pairs (pair k of each camera's 6).
+  T* acc = reinterpret_cast<T*>(product_smem);
   using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-  T2* pws = reinterpret_cast<T2*>(acc + ((m + 1) & ~1u));
-  for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) acc[j] = 0;
-  const uint32_t C = P.C;
+  T2* pws = reinterpret_cast<T2*>(reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, sizeof(T)));
+  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) acc[j] = T(0);
+  if (threadIdx.x == 0) focal_acc = 0;
   if (STAGED)
     for (uint32_t j = threadIdx.x; j < 3 * C; j += blockDim.x) {
       const uint32_t c = j / 3, k = j % 3;
@@ -688,14 +691,14 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      double* ac = acc + c;
-      atomicAdd(ac, -double(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + C, -double(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2 * C, -double(f.q[0] * h1 - f.q[1] * h0));
+      T* ac = acc + c;
+      atomicAdd(ac, -(f.q[1] * h2 - f.q[2] * h1));
+      atomicAdd(ac + C, -(f.q[2] * h0 - f.q[0] * h2));
+      atomicAdd(ac + 2 * C, -(f.q[0] * h1 - f.q[1] * h0));
       if (!directional(P, pt)) {
-        atomicAdd(ac + 3 * C, -double(h0));
-        atomicAdd(ac + 4 * C, -double(h1));
-        atomicAdd(ac + 5 * C, -double(h2));
+        atomicAdd(ac + 3 * C, -h0);
+        atomicAdd(ac + 4 * C, -h1);
+        atomicAdd(ac + 5 * C, -h2);
       }
       continue;
     }
@@ -742,34 +745,34 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      double* ac = acc + c;
-      atomicAdd(ac, -double(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + C, -double(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2 * C, -double(f.q[0] * h1 - f.q[1] * h0));
+      T* ac = acc + c;
+      atomicAdd(ac, -(f.q[1] * h2 - f.q[2] * h1));
+      atomicAdd(ac + C, -(f.q[2] * h0 - f.q[0] * h2));
+      atomicAdd(ac + 2 * C, -(f.q[0] * h1 - f.q[1] * h0));
       if (!directional(P, p0)) {
-        atomicAdd(ac + 3 * C, -double(h0));
-        atomicAdd(ac + 4 * C, -double(h1));
-        atomicAdd(ac + 5 * C, -double(h2));
+        atomicAdd(ac + 3 * C, -h0);
+        atomicAdd(ac + 4 * C, -h1);
+        atomicAdd(ac + 5 * C, -h2);
       }
     }
   }
   if (SHARED) {
     for (int d = 16; d > 0; d >>= 1) ef += __shfl_xor_sync(kFull, ef, d);
-    if (lane == 0) atomicAdd(acc + (m - 1), -ef);
+    if (lane == 0) atomicAdd(&focal_acc, -ef);
   }
   __syncthreads();
   // Rotate each camera's sums into its axes and write this block's partial row.
   double* out = P.acc_part + size_t(blockIdx.x) * m;
   for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
     double a[6];
-    for (int j = 0; j < 6; j++) a[j] = acc[j * C + c];
+    for (int j = 0; j < 6; j++) a[j] = double(acc[j * C + c]);
     const double* R = P.poses + 12 * size_t(c);
     for (int r = 0; r < 3; r++) {
       out[6 * c + r] = R[3 * r] * a[0] + R[3 * r + 1] * a[1] + R[3 * r + 2] * a[2];
       out[6 * c + 3 + r] = R[3 * r] * a[3] + R[3 * r + 1] * a[4] + R[3 * r + 2] * a[5];
     }
   }
-  if (SHARED && threadIdx.x == 0) out[m - 1] = acc[m - 1];
+  if (SHARED && threadIdx.x == 0) out[m - 1] = focal_acc;
 }
 
 // The column sums of the one-pass product's partial rows (fixed order), then the camera rows of
@@ -1364,24 +1367,23 @@ uint32_t product_finish_blocks(const Params& p) {
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
-uint32_t product_max_unknowns() { return (227 * 1024) / sizeof(double) - 64; }
+uint32_t product_max_unknowns() { return uint32_t(kStagedSmemLimit / sizeof(double)) - 64; }
 
 // The direction is staged in shared memory when the camera sums and it fit one block.
 bool product_staged(const Params& p) {
   const size_t word = p.F32 ? sizeof(float) : sizeof(double);
-  return size_t((p.m + 1) & ~1u) * sizeof(double) + 6 * size_t(p.C) * word <= size_t(kStagedSmemLimit);
+  return product_sums_bytes(p.C, word) + 6 * size_t(p.C) * word <= size_t(kStagedSmemLimit);
 }
 
 size_t product_smem_bytes(const Params& p) {
   const size_t word = p.F32 ? sizeof(float) : sizeof(double);
-  return product_staged(p) ? size_t((p.m + 1) & ~1u) * sizeof(double) + 6 * size_t(p.C) * word
-                           : size_t(p.m) * sizeof(double);
+  return product_sums_bytes(p.C, word) + (product_staged(p) ? 6 * size_t(p.C) * word : 0);
 }
 
 int product_threads(const Params& p) { return product_staged(p) ? kStagedThreads : kProductThreads; }
 
 cudaError_t configure_kernels() {
-  const int bytes = 227 * 1024;
+  const int bytes = kStagedSmemLimit;  // the products also hold a few static bytes
   cudaError_t e = cudaSuccess;
   auto set = [&](const void* f) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

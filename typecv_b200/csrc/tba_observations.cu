@@ -5,10 +5,11 @@
 //   k_obs_project   per observation: project the point in its camera; an inlier when the
 //                   projection is in the model's domain and its error is within the threshold
 //                   (projectIndexedObservations)
-//   k_obs_depth     per track (only with a depth bound), a group of 8 lanes per track: the
-//                   linearised depth sensitivity of the track's point to independent pixel noise,
-//                   from its inlier observations with the poses and intrinsics fixed; a track above
-//                   the bound loses all its inliers (filterIndexedObservationDepth, stableDepth)
+//   k_obs_depth     per track (only with a depth bound): the linearised depth sensitivity of the
+//                   track's point to independent pixel noise, from its inlier observations with the
+//                   poses and intrinsics fixed; a track above the bound loses all its inliers
+//                   (filterIndexedObservationDepth, stableDepth).  One thread per track: groups of
+//                   8 lanes per track measured slower (fewer independent tracks in flight per warp)
 //   k_obs_partials  the inlier error sum and count of each run of 64 observations, each run summed
 //                   in order (indexedObservationPartials), then k_obs_summary sums the runs in a
 //                   fixed tree (observationSummary)
@@ -54,85 +55,61 @@ __global__ void __launch_bounds__(256) k_obs_project(ObsParams A) {
   }
 }
 
-// stableDepth and filterIndexedObservationDepth for one track, by a group of kDepthGroup lanes: each
-// lane takes every kDepthGroup-th observation of the track.  The information matrix of the point
-// from the inlier observations (unweighted point Jacobians) is summed over the group, then each
-// inlier's variance of its camera-frame depth, sigma_z^2 = a^T A^-1 a with a the camera's optical
-// axis, is held against the relative bound noise * sigma_z / z.  A track with a projection outside
-// the model's domain, a singular matrix or a bound exceeded loses all its inliers.  (The reference
-// runs one track per thread and sums in observation order; the group's tree sums differ from it by
-// rounding only.)
-constexpr int kDepthGroup = 8;
-
-__device__ inline double group_sum(double v, unsigned mask) {
-#pragma unroll
-  for (int d = kDepthGroup / 2; d > 0; d >>= 1) v += __shfl_xor_sync(mask, v, d);
-  return v;
-}
-
-__global__ void __launch_bounds__(256) k_obs_depth(ObsParams A) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t h = t / kDepthGroup;
-  const uint32_t sub = t % kDepthGroup;
-  const unsigned gmask = 0xFFu << ((threadIdx.x & 31) & ~uint32_t(kDepthGroup - 1));
-  if (h >= A.P) return;  // whole groups: P is per group
-  const uint32_t start = A.offsets[h], end = A.offsets[h + 1];
-  if (sub == 0) A.flags[A.M + h] = 0;
-  uint32_t accepted = 0;
-  for (uint32_t i = start + sub; i < end; i += kDepthGroup) accepted += A.flags[i] != 0;
-  if (__reduce_add_sync(gmask, accepted) < 2) return;
-  const double* X = A.points + 3 * size_t(A.indices[2 * size_t(start) + 1]);
-  double M[6] = {0, 0, 0, 0, 0, 0};  // upper triangle: 00 01 02 11 12 22
-  bool bad = false;
-  for (uint32_t i = start + sub; i < end; i += kDepthGroup) {
+// stableDepth: the information matrix of the point from the inlier observations (unweighted point
+// Jacobians), then for each inlier the variance of its camera-frame depth, sigma_z^2 = a^T A^-1 a
+// with a the camera's optical axis, against the relative bound noise * sigma_z / z.
+__device__ bool obs_stable_depth(const ObsParams& A, uint32_t start, uint32_t end, const double* X) {
+  double M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t count = 0;
+  for (uint32_t i = start; i < end; i++) {
     if (A.flags[i] == 0) continue;
+    count++;
     double pose[12], q[3], pixel[2], du[3], dv[3];
     Camera k;
     obs_camera(A, i, pose, k);
     obs_transform(pose, X, q);
-    if (!project(k, q, pixel, du, dv)) {
-      bad = true;
-      continue;
-    }
+    if (!project(k, q, pixel, du, dv)) return false;
     for (int row = 0; row < 2; row++) {
       const double* g = row == 0 ? du : dv;
       const double J[3] = {g[0] * pose[0] + g[1] * pose[3] + g[2] * pose[6],
                            g[0] * pose[1] + g[1] * pose[4] + g[2] * pose[7],
                            g[0] * pose[2] + g[1] * pose[5] + g[2] * pose[8]};
-      M[0] += J[0] * J[0];
-      M[1] += J[0] * J[1];
-      M[2] += J[0] * J[2];
-      M[3] += J[1] * J[1];
-      M[4] += J[1] * J[2];
-      M[5] += J[2] * J[2];
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) M[3 * r + c] += J[r] * J[c];
     }
   }
-  bool reject = __any_sync(gmask, bad);
-  if (!reject) {
-    for (int k = 0; k < 6; k++) M[k] = group_sum(M[k], gmask);
-    const double Mf[9] = {M[0], M[1], M[2], M[1], M[3], M[4], M[2], M[4], M[5]};
-    bool fail = false;
-    for (uint32_t i = start + sub; i < end; i += kDepthGroup) {
-      if (A.flags[i] == 0) continue;
-      double pose[12], q[3], s[3];
-      Camera k;
-      obs_camera(A, i, pose, k);
-      const double axis[3] = {pose[6], pose[7], pose[8]};
-      obs_transform(pose, X, q);
-      if (!solve3_spd(Mf, axis, s) || !(q[2] > 0)) {
-        fail = true;
-        continue;
-      }
-      const double variance = axis[0] * s[0] + axis[1] * s[1] + axis[2] * s[2];
-      if (!(variance >= 0) || !(A.noise * sqrt(variance) / q[2] <= A.max_relative_depth)) fail = true;
-    }
-    reject = __any_sync(gmask, fail);
+  if (count < 2) return false;
+  for (uint32_t i = start; i < end; i++) {
+    if (A.flags[i] == 0) continue;
+    double pose[12], q[3], s[3];
+    Camera k;
+    obs_camera(A, i, pose, k);
+    const double axis[3] = {pose[6], pose[7], pose[8]};
+    obs_transform(pose, X, q);
+    if (!solve3_spd(M, axis, s) || !(q[2] > 0)) return false;
+    const double variance = axis[0] * s[0] + axis[1] * s[1] + axis[2] * s[2];
+    if (!(variance >= 0)) return false;
+    const double relative = A.noise * sqrt(variance) / q[2];
+    if (!(relative <= A.max_relative_depth)) return false;
   }
-  if (!reject) return;
-  if (sub == 0) A.flags[A.M + h] = 1;
-  for (uint32_t i = start + sub; i < end; i += kDepthGroup) {
-    A.flags[i] = 0;
-    A.errors[i] = 0;
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_obs_depth(ObsParams A) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= A.P) return;
+  const uint32_t start = A.offsets[h], end = A.offsets[h + 1];
+  A.flags[A.M + h] = 0;
+  if (end <= start) return;
+  uint32_t accepted = 0;
+  for (uint32_t i = start; i < end; i++) accepted += A.flags[i] != 0;
+  if (accepted < 2) return;
+  if (!obs_stable_depth(A, start, end, A.points + 3 * size_t(A.indices[2 * size_t(start) + 1]))) {
+    A.flags[A.M + h] = 1;
+    for (uint32_t i = start; i < end; i++) {
+      A.flags[i] = 0;
+      A.errors[i] = 0;
+    }
   }
 }
 
@@ -180,7 +157,7 @@ __global__ void __launch_bounds__(1024) k_obs_summary(ObsParams A) {
 
 void launch_observations(const ObsParams& a, cudaStream_t s) {
   if (a.M) k_obs_project<<<(a.M + 255) / 256, 256, 0, s>>>(a);
-  if (a.guarded && a.P) k_obs_depth<<<uint32_t((uint64_t(a.P) * kDepthGroup + 255) / 256), 256, 0, s>>>(a);
+  if (a.guarded && a.P) k_obs_depth<<<(a.P + 127) / 128, 128, 0, s>>>(a);
   const uint32_t runs = (a.M + 63) / 64;
   if (runs) k_obs_partials<<<(runs + 255) / 256, 256, 0, s>>>(a);
   k_obs_summary<<<1, 1024, 0, s>>>(a);
