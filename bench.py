@@ -333,6 +333,46 @@ def time_form(args, world, local, scene, precision, iterations):
     return reports, walls, out.copy(), clk
 
 
+def time_resident(args, world, local, scene, precision, iterations):
+    """Row f2: the same solve through a resident scene (tba_scene_create once; per step
+    tba_scene_write of the initial poses and points, then tba_scene_adjust, which reads back only the
+    state words).  Returns LM steps/s end to end (host wall time) and on the device."""
+    import torch
+    import typecv_b200 as tb
+    from typecv_b200 import _lib
+    from typecv_b200.resident import ResidentScene
+    s_np, i_np = scene.packed()
+    C, P = scene.C, scene.P
+    poses = pinned_like(np.ascontiguousarray(s_np[:12 * C]), torch)
+    points = pinned_like(np.ascontiguousarray(s_np[12 * C:12 * C + 3 * P]), torch)
+    ctl = tb.make_control(C, P, scene.M, anchor=0, scale_view=1, iterations=iterations, shared_focal=True,
+                          huber=2.0, tolerance=1e-6, precision=precision)
+    dev = tb.ShadeDevice.open(local)
+    try:
+        with ResidentScene(dev, ctl, s_np, i_np) as rs:
+            for _ in range(max(args.warmup, 1)):
+                rs.write(poses, points)
+                rs.adjust()
+            walls, reps = [], []
+            barrier(world)
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                rs.write(poses, points)
+                _, state, rep = rs.adjust()
+                walls.append(time.perf_counter() - t0)
+                reps.append(rep)
+            barrier(world)
+    finally:
+        dev.close()
+    lm = sum_over_ranks(world, sum(r["lm_iterations"] for r in reps))
+    wall_s = max_over_ranks(world, sum(walls))
+    solve_s = max_over_ranks(world, sum(r["solve_ms"] for r in reps) / 1000)
+    return {"e2e": lm / wall_s, "value": lm / solve_s, "unit": UNIT, "final_cost": float(state[6]),
+            "h2d_bytes_per_step": 8 * (12 * C + 3 * P), "d2h_bytes_per_step": 8 * len(state),
+            "check_ms": reps[-1].get("check_ms", 0.0),
+            "note": "tba_scene_write of the initial poses and points + tba_scene_adjust per step, mixed form"}
+
+
 def form_summary(world, scene, reports, walls, out):
     solve_s = sum(r["solve_ms"] for r in reports) / 1000
     lm = sum(r["lm_iterations"] for r in reports)
@@ -375,6 +415,8 @@ def run_single(args, world, rank, local):
         prec = _lib.TBA_PRECISION_MIXED if form == "mixed" else _lib.TBA_PRECISION_FP64
         reports, walls, out, clk = time_form(args, world, local, scene, prec, iterations)
         results[form] = (reports, walls, out, clk, form_summary(world, scene, reports, walls, out))
+    if args.config == "cfg2" and forms[0] == "mixed":
+        results["resident"] = time_resident(args, world, local, scene, _lib.TBA_PRECISION_MIXED, iterations)
     if rank != 0:
         return
     head = forms[0]
@@ -403,6 +445,8 @@ def run_single(args, world, rank, local):
                         "gpu_launches": sum(r["kernel_launches"] for r in r64)}
         line["mixed_vs_fp64"] = {"lm_steps_ratio": summ["value"] / s64["value"],
                                  "final_cost_rel_diff": abs(summ["final_cost"] - s64["final_cost"]) / s64["final_cost"]}
+    if head == "mixed" or len(forms) == 2:
+        line["resident"] = results.get("resident")
     if world == 1 and not args.no_cpu_baseline:
         dt, ran, threads = cpu_baseline_run(scene, 1)
         line["cpu_baseline"] = {"value": ran / dt, "unit": UNIT, "cores": threads, "kind": "port",
