@@ -14,8 +14,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtba.so")
-SOURCES = ["tba_kernels.cu", "tba_batch.cu", "tba_adjoint.cu", "tba_observations.cu", "tba_api.cu", "tba_noalloc.cu"]
-HEADERS = ["tba_math.cuh", "tba_engine.cuh", "tba_warp.cuh", "tba_batch.cuh", "tba_adjoint.cuh", "tba_observations.cuh"]
+SOURCES = ["tba_kernels.cu", "tba_batch.cu", "tba_adjoint.cu", "tba_observations.cu", "tba_checks.cu", "tba_api.cu",
+           "tba_noalloc.cu"]
+HEADERS = ["tba_math.cuh", "tba_engine.cuh", "tba_warp.cuh", "tba_batch.cuh", "tba_adjoint.cuh", "tba_observations.cuh",
+           "tba_checks.cuh"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
 

@@ -24,6 +24,7 @@
 #include "tba_adjoint.cuh"
 #include "tba_batch.cuh"
 #include "tba_engine.cuh"
+#include "tba_checks.cuh"
 #include "tba_observations.cuh"
 
 using tba::Params;
@@ -215,6 +216,63 @@ void check_scene(const tba_control* c, const double* scene, size_t len) {
       argument("Camera exceeds the supported GPU geometry bounds");
 }
 
+// The O(1) and O(C) parts of check_index and check_scene, on the host, with the message each would
+// raise (null where it passes); the O(M) and O(P) parts run on the device after the upload
+// (tba_checks.cu), and raise_checks reports the failure that check_index then check_scene, in
+// their order, would meet first.
+struct HostChecks {
+  const char* point_ends = nullptr;     // before the per-point checks
+  const char* camera_ends = nullptr;    // after the observation cameras
+  const char* camera_offsets = nullptr;
+  const char* activity = nullptr;       // after the camera lists
+  const char* camera_bounds = nullptr;  // after the scene values
+};
+
+HostChecks host_checks(const tba_control* c, const uint32_t* index, const double* scene) {
+  HostChecks h;
+  const uint64_t C = c->cameras, P = c->points, M = c->observations;
+  const uint32_t* ps = index + 2 * M;
+  const uint32_t* cs = ps + P + 1;
+  const uint32_t* active = cs + C + 1 + M;
+  if (ps[0] != 0 || ps[P] != M) h.point_ends = "Invalid GPU BA index: point offsets do not cover the observations";
+  if (cs[0] != 0 || cs[C] != M) h.camera_ends = "Invalid GPU BA index: camera offsets do not cover the observations";
+  for (uint64_t cam = 0; cam < C && !h.camera_offsets; cam++)
+    if (cs[cam + 1] < cs[cam] || cs[cam + 1] > M)
+      h.camera_offsets = "Invalid GPU BA index: camera offsets decrease or exceed the observations";
+  uint32_t fixed = 0;
+  for (uint64_t cam = 0; cam < C && !h.activity; cam++) {
+    if (active[cam] > 1) h.activity = "Invalid GPU BA index: camera activity flags must be 0 or 1";
+    fixed += active[cam] == 0;
+  }
+  if (!h.activity && active[c->anchor] != 0) h.activity = "Invalid GPU BA gauge cameras: the anchor must be fixed";
+  if (!h.activity && fixed > 1 && active[c->scale_view] != 0) h.activity = "Local GPU BA scale camera must be fixed";
+  const double* k = scene + 12 * size_t(C) + 3 * size_t(P);
+  for (uint64_t cam = 0; cam < C && !h.camera_bounds; cam++, k += 6)
+    if (!(k[0] > 0 && k[1] > 0) || k[0] < 1e-6 || k[1] < 1e-6 || k[0] > 1e6 || k[1] > 1e6 ||
+        std::max(std::fabs(k[2]), std::fabs(k[3])) > 1e9 || std::max(std::fabs(k[4]), std::fabs(k[5])) > 1)
+      h.camera_bounds = "Camera exceeds the supported GPU geometry bounds";
+  return h;
+}
+
+void raise_checks(const HostChecks& h, const unsigned long long* keys) {
+  const unsigned long long none = ~0ull;
+  if (h.point_ends) argument(h.point_ends);
+  if (keys[tba::CK_POINTS] != none) {
+    static const char* const messages[3] = {"Invalid GPU BA index: point offsets exceed the observations",
+                                            "Landmarks require at least two observations",
+                                            "Invalid GPU BA index: observation point does not match the point offsets"};
+    argument(messages[keys[tba::CK_POINTS] & 3]);
+  }
+  if (keys[tba::CK_CAMERA] != none) argument("Invalid GPU BA index: observation camera out of range");
+  if (h.camera_ends) argument(h.camera_ends);
+  if (h.camera_offsets) argument(h.camera_offsets);
+  if (keys[tba::CK_LISTS] != none)
+    argument("Invalid GPU BA index: camera observation lists are not the observations of each camera");
+  if (h.activity) argument(h.activity);
+  if (keys[tba::CK_SCENE] != none) argument("GPU BA input exceeds supported coordinate bounds");
+  if (h.camera_bounds) argument(h.camera_bounds);
+}
+
 // Runs of whole points of at most 32 observations; a longer point is a run of its own.
 std::vector<uint32_t> build_tasks(const uint32_t* ps, uint32_t P) {
   std::vector<uint32_t> tasks;
@@ -304,6 +362,10 @@ struct SolveIO {
   const HostPlan* plan = nullptr;
   double* writeback = nullptr;
   double* state = nullptr;
+  // When set, the O(M) checks run on the device right after the upload and a failure is raised
+  // (with these host-side results, in the serial order) before any solver kernel runs.
+  const HostChecks* checks = nullptr;
+  double* check_ms = nullptr;  // receives the device checks' host wall time
 };
 
 void solve(tba_device* d, const tba_control* ctl, const double* scene, const uint32_t* index,
@@ -369,7 +431,8 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_vec = L.take<double>(5 * size_t(m)), o_blk = L.take<double>(4 * size_t(fblocks)),
                o_scal = L.take<double>(size_t(tba::kScalarPartials) * p.task_blocks),
                o_cost = L.take<double>(4 * size_t(p.task_blocks)), o_ticket = L.take<uint32_t>(8),
-               o_state = L.take<double>(tba::S_WORDS), o_out = L.take<double>(12 * size_t(C) + 3 * size_t(P) + 27);
+               o_state = L.take<double>(tba::S_WORDS), o_out = L.take<double>(12 * size_t(C) + 3 * size_t(P) + 27),
+               o_keys = L.take<unsigned long long>(tba::CK_WORDS);
   if (d->capacity < L.bytes) {
     if (d->arena) CUDA_TRY(cudaFree(d->arena));
     d->arena = nullptr;
@@ -458,6 +521,37 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   up_host(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
   up_host(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
   CUDA_TRY(cudaEventRecord(e_up, s));
+  if (io.checks) {
+    const auto c0 = std::chrono::steady_clock::now();
+    tba::CheckParams cp{};
+    cp.C = C;
+    cp.P = P;
+    cp.M = M;
+    cp.index = dindex;
+    cp.seg[0] = p.poses;
+    cp.seg[1] = p.points;
+    cp.seg[2] = p.cams;
+    cp.seg[3] = p.pixels;
+    cp.base[0] = 0;
+    cp.len[0] = 12 * uint64_t(C);
+    cp.base[1] = cp.len[0];
+    cp.len[1] = 3 * uint64_t(P);
+    cp.base[2] = cp.base[1] + cp.len[1];
+    cp.len[2] = 6 * uint64_t(C);
+    cp.base[3] = cp.base[2] + cp.len[2];
+    cp.len[3] = 2 * uint64_t(M);
+    cp.claims = p.cm_point;  // scratch until k_setup writes the camera-major point index
+    cp.keys = reinterpret_cast<unsigned long long*>(a + o_keys);
+    cp.lists = !io.checks->camera_ends && !io.checks->camera_offsets;
+    CUDA_TRY(tba::launch_checks(cp, d->sms, s));
+    CUDA_TRY(cudaMemcpyAsync(d->pinned, cp.keys, tba::CK_WORDS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    unsigned long long keys[tba::CK_WORDS];
+    std::memcpy(keys, d->pinned, sizeof keys);
+    if (io.check_ms)
+      *io.check_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
+    raise_checks(*io.checks, keys);
+  }
 
   uint32_t launches = 0, lm_done = 0, refinements = 0;
   // Event pairs around the Schur products; after the solve, only the products that ran PCG steps
@@ -1272,12 +1366,15 @@ tba_status tba_bundle_adjust(tba_device* d, const tba_control* control, const do
     if (output_len < tba_output_size(control)) argument("Invalid GPU BA output array length");
     if (uint64_t(3) * control->observations + control->points + 2ull * control->cameras + 2 > 0xffffffffull)
       argument("GPU BA scene dimensions exceed integer index bounds");
+    // The O(C) checks here, the O(M) ones on the device after the upload (before any solver kernel).
     const auto t0 = std::chrono::steady_clock::now();
-    check_index(control, index);
-    check_scene(control, scene, scene_len);
-    const double check_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    const HostChecks hc = host_checks(control, index, scene);
+    double check_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     CUDA_TRY(cudaSetDevice(d->ordinal));
-    solve(d, control, scene, index, output, report);
+    SolveIO io;
+    io.checks = &hc;
+    io.check_ms = &check_ms;
+    solve(d, control, scene, index, output, report, io);
     if (report) report->check_ms = check_ms;
   } catch (const Fail& f) {
     d->error = f.message;
