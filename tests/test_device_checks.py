@@ -103,4 +103,7 @@ def test_a_valid_problem_passes_and_reports_its_check_time(device, problem):
     with pytest.raises(tb.RangeError):
         tb.solve_packed(device, ctl, bad_s, bad_i)
     out2, _ = tb.solve_packed(device, ctl, s, i)
-    assert np.array_equal(out, out2)
+    # Same solve: the shared-memory atomics of the product commute only up to rounding.
+    base = 12 * sc.C + 3 * sc.P
+    assert abs(out2[base + 6] - out[base + 6]) <= 1e-9 * out[base + 6]
+    assert np.max(np.abs(out2[:base] - out[:base])) < 1e-7
