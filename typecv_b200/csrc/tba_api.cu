@@ -374,13 +374,13 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const uint32_t C = ctl->cameras, P = ctl->points, M = ctl->observations;
   const bool shared = ctl->shared_focal != 0;
   const uint32_t m = 6 * C + (shared ? 1 : 0);
-  HostPlan own;
-  if (!io.plan) own = make_plan(ctl, index, d->sms);
-  const HostPlan& plan = io.plan ? *io.plan : own;
-  const std::vector<uint32_t>& tasks = plan.tasks;
-  const Chunks& chunks = plan.chunks;
-  const uint32_t ntasks = uint32_t(tasks.size() - 1), nchunks = uint32_t(chunks.cam.size());
-  const uint32_t fixed = plan.fixed;
+  // The host schedules (warp tasks, camera chunks) are built while the problem arrays upload: the
+  // workspace is laid out with bounds of their sizes (at most P + 1 task starts; at most
+  // C + M / 128 + 1 chunks, chunks being at least 128 observations long).  A problem whose camera
+  // offsets fail the host checks gets no schedule; its checks fail before any kernel runs.
+  const bool plannable = !io.checks || (!io.checks->camera_ends && !io.checks->camera_offsets);
+  const uint64_t max_tasks = io.plan ? io.plan->tasks.size() : uint64_t(P) + 1;
+  const uint64_t max_chunks = io.plan ? io.plan->chunks.cam.size() : uint64_t(C) + M / 128 + 1;
 
   Params p{};
   p.C = C;
@@ -390,7 +390,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.m = m;
   p.anchor = ctl->anchor;
   p.scale_view = ctl->scale_view;
-  p.normalize_scale = fixed == 1;
   p.shared = shared;
   p.huber = ctl->huber;
   p.tol = ctl->cg_tolerance;
@@ -398,9 +397,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   // The mixed form's inner PCG runs stop at a relative residual the FP32 product can reach; the
   // FP64 refinement then measures the true residual against the caller's tolerance.
   p.tol_inner = ctl->precision == TBA_PRECISION_MIXED ? std::max(ctl->cg_tolerance, 1e-6) : ctl->cg_tolerance;
-  p.ntasks = ntasks;
-  p.nchunks = nchunks;
-  p.task_blocks = std::max<uint32_t>(1, std::min<uint32_t>(4 * d->sms, (ntasks + 7) / 8));
+  const uint32_t max_task_blocks = std::max<uint32_t>(1, 4 * uint32_t(d->sms));
   const uint32_t fblocks = tba::product_finish_blocks(p);
   // The one-pass product over stored factors when its camera sums fit shared memory; the two-pass
   // recompute form otherwise.  The mixed form stores FP32 factors.
@@ -411,26 +408,26 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.F = nullptr;
   p.F32 = mixed && p.factored ? reinterpret_cast<float*>(1) : nullptr;  // set below; selects the occupancy query
   const int per_sm = p.factored ? tba::product_blocks_per_sm(p) : 1;
-  p.prod_blocks = std::max<uint32_t>(1, std::min<uint32_t>(uint32_t(per_sm * d->sms), (ntasks + 15) / 16));
+  const uint32_t max_prod_blocks = std::max<uint32_t>(1, uint32_t(per_sm * d->sms));
   Layout L;
   const size_t o_poses = L.take<double>(12 * size_t(C)), o_points = L.take<double>(3 * size_t(P)),
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
                o_tposes = L.take<double>(12 * size_t(C)), o_tpoints = L.take<double>(3 * size_t(P)),
                o_index = L.take<uint32_t>(3 * size_t(M) + P + 2 * size_t(C) + 2),
-               o_tasks = L.take<uint32_t>(tasks.size()), o_tobs = L.take<uint32_t>(tasks.size()),
-               o_ccam = L.take<uint32_t>(nchunks),
-               o_cbeg = L.take<uint32_t>(nchunks + 1), o_cfirst = L.take<uint32_t>(C + 1),
+               o_tasks = L.take<uint32_t>(max_tasks), o_tobs = L.take<uint32_t>(max_tasks),
+               o_ccam = L.take<uint32_t>(max_chunks),
+               o_cbeg = L.take<uint32_t>(max_chunks + 1), o_cfirst = L.take<uint32_t>(C + 1),
                o_rlim = L.take<double>(C), o_cmp = L.take<uint32_t>(M), o_cmx = L.take<double>(2 * size_t(M)),
                o_pblk = L.take<double>(12 * size_t(P)), o_y = L.take<double>(4 * size_t(P)),
-               o_cprod = L.take<double>(8 * size_t(nchunks)), o_F = L.take<char>(factor_bytes),
+               o_cprod = L.take<double>(8 * max_chunks), o_F = L.take<char>(factor_bytes),
                o_pw = L.take<double>(6 * size_t(C)), o_xw = L.take<double>(6 * size_t(C)),
-               o_acc = L.take<double>(p.factored ? size_t(p.prod_blocks) * m : 0), o_U = L.take<double>(21 * size_t(C)),
+               o_acc = L.take<double>(p.factored ? size_t(max_prod_blocks) * m : 0), o_U = L.take<double>(21 * size_t(C)),
                o_Minv = L.take<double>(36 * size_t(C)), o_rhs = L.take<double>(6 * size_t(C)),
                o_hcf = L.take<double>(6 * size_t(C)),
-               o_chunk = L.take<double>(size_t(tba::kCameraPartials) * nchunks),
+               o_chunk = L.take<double>(size_t(tba::kCameraPartials) * max_chunks),
                o_vec = L.take<double>(5 * size_t(m)), o_blk = L.take<double>(4 * size_t(fblocks)),
-               o_scal = L.take<double>(size_t(tba::kScalarPartials) * p.task_blocks),
-               o_cost = L.take<double>(4 * size_t(p.task_blocks)), o_ticket = L.take<uint32_t>(8),
+               o_scal = L.take<double>(size_t(tba::kScalarPartials) * max_task_blocks),
+               o_cost = L.take<double>(4 * size_t(max_task_blocks)), o_ticket = L.take<uint32_t>(8),
                o_state = L.take<double>(tba::S_WORDS), o_out = L.take<double>(12 * size_t(C) + 3 * size_t(P) + 27),
                o_keys = L.take<unsigned long long>(tba::CK_WORDS);
   if (d->capacity < L.bytes) {
@@ -515,11 +512,26 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   up(const_cast<double*>(p.cams), scene + 12 * size_t(C) + 3 * size_t(P), 6 * sizeof(double) * C);
   up(const_cast<double*>(p.pixels), scene + 18 * size_t(C) + 3 * size_t(P), 2 * sizeof(double) * M);
   up(dindex, index, sizeof(uint32_t) * (3 * size_t(M) + P + 2 * size_t(C) + 2));
-  up_host(U32(o_tasks), tasks.data(), sizeof(uint32_t) * tasks.size());
-  up_host(U32(o_tobs), plan.task_obs.data(), sizeof(uint32_t) * plan.task_obs.size());
-  up_host(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
-  up_host(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
-  up_host(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
+  // The schedules, built on the host while the copies above run.
+  HostPlan own;
+  if (!io.plan && plannable) own = make_plan(ctl, index, d->sms);
+  const HostPlan& plan = io.plan ? *io.plan : own;
+  const std::vector<uint32_t>& tasks = plan.tasks;
+  const Chunks& chunks = plan.chunks;
+  const uint32_t ntasks = tasks.empty() ? 0 : uint32_t(tasks.size() - 1), nchunks = uint32_t(chunks.cam.size());
+  if (plannable) {
+    if (tasks.size() > max_tasks || nchunks > max_chunks) throw Fail{TBA_ERROR_INTERNAL, "GPU BA schedule exceeds its bound"};
+    up_host(U32(o_tasks), tasks.data(), sizeof(uint32_t) * tasks.size());
+    up_host(U32(o_tobs), plan.task_obs.data(), sizeof(uint32_t) * plan.task_obs.size());
+    up_host(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
+    up_host(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
+    up_host(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
+  }
+  p.normalize_scale = plan.fixed == 1;
+  p.ntasks = ntasks;
+  p.nchunks = nchunks;
+  p.task_blocks = std::max<uint32_t>(1, std::min<uint32_t>(max_task_blocks, (ntasks + 7) / 8));
+  p.prod_blocks = std::max<uint32_t>(1, std::min<uint32_t>(max_prod_blocks, (ntasks + 15) / 16));
   CUDA_TRY(cudaEventRecord(e_up, s));
   if (io.checks) {
     const auto c0 = std::chrono::steady_clock::now();
@@ -551,6 +563,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     if (io.check_ms)
       *io.check_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
     raise_checks(*io.checks, keys);
+    if (!plannable) throw Fail{TBA_ERROR_INTERNAL, "GPU BA checks passed a problem without a schedule"};
   }
 
   uint32_t launches = 0, lm_done = 0, refinements = 0;
