@@ -734,29 +734,50 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
   uint32_t Cmax = 2;
   std::vector<uint32_t> tasks;
   std::vector<uint64_t> task_first(count), task_count(count);
+  // Each problem is checked and scheduled on its own; the problems are spread over host threads and
+  // the failure reported is the one of the first failing problem, as a loop in order would report.
+  std::vector<std::vector<uint32_t>> problem_tasks(count);
+  std::mutex fail_mu;
+  uint32_t fail_at = UINT32_MAX;
+  Fail first_fail{TBA_OK, ""};
+  parallel_ranges(count, 2, [&](uint64_t b, uint64_t e, unsigned) {
+    for (uint64_t k = b; k < e; k++) {
+      try {
+        const tba_batch_problem& q = probs[k];
+        const tba_control c = batch_problem_control(bc, q);
+        check_control(&c);
+        if (q.reserved != 0) argument("Invalid GPU BA batch: reserved field must be 0");
+        if (q.cameras > max_cams)
+          argument("Batched GPU BA problem has " + std::to_string(q.cameras) +
+                   " cameras; the block solver takes at most " + std::to_string(max_cams));
+        if (uint64_t(3) * q.observations + q.points + 2ull * q.cameras + 2 > 0xffffffffull)
+          argument("GPU BA scene dimensions exceed integer index bounds");
+        if (q.scene_offset > scene_len || scene_len - q.scene_offset < tba_scene_size(&c))
+          argument("Invalid GPU BA batch: a scene lies outside the scene array");
+        if (q.index_offset > index_len || index_len - q.index_offset < tba_index_size(&c))
+          argument("Invalid GPU BA batch: an index lies outside the index array");
+        if (q.output_offset > output_len || output_len - q.output_offset < tba_output_size(&c))
+          argument("Invalid GPU BA batch: a result record lies outside the output array");
+        check_index(&c, index + q.index_offset);
+        check_scene(&c, scene + q.scene_offset, tba_scene_size(&c));
+        problem_tasks[k] = build_tasks(index + q.index_offset + 2 * size_t(q.observations), q.points);
+      } catch (const Fail& f) {
+        std::lock_guard<std::mutex> lock(fail_mu);
+        if (k < fail_at) {
+          fail_at = uint32_t(k);
+          first_fail = f;
+        }
+        return;
+      }
+    }
+  });
+  if (fail_at != UINT32_MAX) throw first_fail;
   for (uint32_t k = 0; k < count; k++) {
-    const tba_batch_problem& q = probs[k];
-    const tba_control c = batch_problem_control(bc, q);
-    check_control(&c);
-    if (q.reserved != 0) argument("Invalid GPU BA batch: reserved field must be 0");
-    if (q.cameras > max_cams)
-      argument("Batched GPU BA problem has " + std::to_string(q.cameras) + " cameras; the block solver takes at most " +
-               std::to_string(max_cams));
-    if (uint64_t(3) * q.observations + q.points + 2ull * q.cameras + 2 > 0xffffffffull)
-      argument("GPU BA scene dimensions exceed integer index bounds");
-    if (q.scene_offset > scene_len || scene_len - q.scene_offset < tba_scene_size(&c))
-      argument("Invalid GPU BA batch: a scene lies outside the scene array");
-    if (q.index_offset > index_len || index_len - q.index_offset < tba_index_size(&c))
-      argument("Invalid GPU BA batch: an index lies outside the index array");
-    if (q.output_offset > output_len || output_len - q.output_offset < tba_output_size(&c))
-      argument("Invalid GPU BA batch: a result record lies outside the output array");
-    check_index(&c, index + q.index_offset);
-    check_scene(&c, scene + q.scene_offset, tba_scene_size(&c));
-    const std::vector<uint32_t> t = build_tasks(index + q.index_offset + 2 * size_t(q.observations), q.points);
+    const std::vector<uint32_t>& t = problem_tasks[k];
     task_first[k] = tasks.size();
     task_count[k] = t.size() - 1;
     tasks.insert(tasks.end(), t.begin(), t.end());
-    Cmax = std::max(Cmax, q.cameras);
+    Cmax = std::max(Cmax, probs[k].cameras);
   }
   // Result records must not overlap: the device writes each one whole.
   std::vector<uint32_t> by_out(count);
