@@ -1537,21 +1537,31 @@ tba_status tba_evaluate_observations(tba_device* d, const tba_observation_contro
     if (guarded) {
       if (!offsets || offsets_len < P + 1) argument("Invalid GPU observation arrays: track offsets");
       if (offsets[0] != 0 || offsets[P] != M) argument("Invalid GPU observation arrays: track offsets");
-      for (uint64_t h = 0; h < P; h++) {
-        if (offsets[h + 1] < offsets[h]) argument("Invalid GPU observation arrays: track offsets");
-        for (uint64_t i = offsets[h]; i < offsets[h + 1]; i++)
-          if (indices[2 * i + 1] != h) argument("Invalid GPU observation arrays: track offsets");
-      }
+      FirstFailure tf;
+      parallel_ranges(P, 1u << 16, [&](uint64_t b, uint64_t e, unsigned) {
+        for (uint64_t h = b; h < e; h++) {
+          if (offsets[h + 1] < offsets[h] || offsets[h + 1] > M)
+            return tf.record(h, "Invalid GPU observation arrays: track offsets");
+          for (uint64_t i = offsets[h]; i < offsets[h + 1]; i++)
+            if (indices[2 * i + 1] != h) return tf.record(h, "Invalid GPU observation arrays: track offsets");
+        }
+      });
+      tf.raise();
     }
-    auto bounded = [](const double* v, uint64_t n) {
-      for (uint64_t i = 0; i < n; i++) {
-        const double x = v[i];
-        if (!std::isfinite(x) || std::fabs(x) > 1e9 || (x != 0 && std::fabs(x) < 1e-30)) return false;
-      }
-      return true;
+    FirstFailure bf;
+    auto bounded = [&](const double* v, uint64_t n, uint64_t base) {
+      parallel_ranges(n, 1u << 18, [&](uint64_t b, uint64_t e, unsigned) {
+        for (uint64_t i = b; i < e; i++) {
+          const double x = v[i];
+          if (!std::isfinite(x) || std::fabs(x) > 1e9 || (x != 0 && std::fabs(x) < 1e-30))
+            return bf.record(base + i, "Invalid GPU scene coordinate bounds");
+        }
+      });
     };
-    if (!bounded(cameras, 18 * C) || !bounded(points, 3 * P) || !bounded(pixels, 2 * M))
-      argument("Invalid GPU scene coordinate bounds");
+    bounded(cameras, 18 * C, 0);
+    bounded(points, 3 * P, 18 * C);
+    bounded(pixels, 2 * M, 18 * C + 3 * P);
+    bf.raise();
     CUDA_TRY(cudaSetDevice(d->ordinal));
     evaluate_observations(d, oc, cameras, points, pixels, indices, offsets, flags, summary, report);
   } catch (const Fail& f) {
