@@ -436,15 +436,23 @@ def run_single(args, world, rank, local):
         "gpu_launches": sum(r["kernel_launches"] for r in reports),
     }
     if head == "mixed":
-        line["mixed"] = {"refinements": summ["refinements"], "cg_iterations": summ["cg_iterations"]}
+        base = 12 * scene.C + 3 * scene.P
+        line["mixed"] = {"refinements": summ["refinements"], "cg_iterations": summ["cg_iterations"],
+                         "pcg_failures": int(out[base + 17])}
     if len(forms) == 2:
         r64, _, _, clk64, s64 = results["fp64"]
         line["fp64"] = {"value": s64["value"], "e2e": s64["e2e"], "pcg_iterations_per_s": s64["pcg_iterations_per_s"],
                         "final_cost": s64["final_cost"], "final_rmse_px": s64["final_rmse_px"],
                         "roofline": roofline(scene, r64, "fp64"), "clocks": clk64,
                         "gpu_launches": sum(r["kernel_launches"] for r in r64)}
+        out64 = results["fp64"][2]
+        n = 12 * scene.C + 3 * scene.P
         line["mixed_vs_fp64"] = {"lm_steps_ratio": summ["value"] / s64["value"],
-                                 "final_cost_rel_diff": abs(summ["final_cost"] - s64["final_cost"]) / s64["final_cost"]}
+                                 "final_cost_rel_diff": abs(summ["final_cost"] - s64["final_cost"]) / s64["final_cost"],
+                                 "max_pose_diff": float(np.max(np.abs(out[:12 * scene.C] - out64[:12 * scene.C]))),
+                                 "max_point_diff": float(np.max(np.abs(out[12 * scene.C:n] - out64[12 * scene.C:n]))),
+                                 "final_rmse_diff_px": abs(summ["final_rmse_px"] - s64["final_rmse_px"])}
+        line["fp64"]["pcg"] = {"iterations": s64["cg_iterations"], "failures": int(out64[n + 17])}
     if head == "mixed" or len(forms) == 2:
         line["resident"] = results.get("resident")
     if world == 1 and not args.no_cpu_baseline:
