@@ -195,34 +195,39 @@ def init_dist(args):
     return world, rank, local
 
 
+def _reduce_device():
+    """Where the reductions' one-word tensors live: the GPU under NCCL, the host under gloo."""
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def barrier(world):
     import torch
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+
+
+def _all_reduce(world, value, op):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device())
+    dist.all_reduce(t, op=op)
+    return float(t.item())
 
 
 def max_over_ranks(world, value):
-    if world == 1:
-        return value
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _all_reduce(world, value, dist.ReduceOp.MAX)
 
 
 def sum_over_ranks(world, value):
-    if world == 1:
-        return value
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
-
-
+    return _all_reduce(world, value, dist.ReduceOp.SUM)
 
 
 def finish_dist(world):
