@@ -253,3 +253,23 @@ def test_mixed_precision_through_the_operator(device):
     assert mixed["diagnostics"]["finalCost"] < 1e-7 and mixed["diagnostics"]["finalRmsePx"] < 1e-4
     assert abs(mixed["reconstruction"]["views"][0]["camera"]["fx"] - jf["truth"]["views"][0]["camera"]["fx"]) < 0.001
     assert abs(mixed["diagnostics"]["finalCost"] - fp64["diagnostics"]["finalCost"]) < 1e-7
+
+
+def test_beyond_the_shared_memory_limit_the_two_pass_engine_matches_the_oracle(device):
+    # 5,000 cameras: 30,000+ camera unknowns do not fit one block's shared memory, so the engine
+    # takes the two-pass recompute product (report engine 1) in both forms.
+    scene = S.helix_scene(seed=31, cameras=5000, points=20000, laps=12, pitch=0.3)
+    s, i = scene.packed()
+    packed = {"C": scene.C, "P": scene.P, "M": scene.M, "scene": s, "index": i}
+    ctl = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, iterations=3, shared_focal=True)
+    out, rep = tb.solve_packed(device, ctl, s, i)
+    assert rep["engine"] == 1 and rep["product_blocks"] == 0
+    ref = ob.gpu_operator_packed(packed, 0, 1, iterations=3, huber=2.0, max_cg=ctl.max_cg, shared=True)
+    base = 12 * scene.C + 3 * scene.P
+    assert abs(out[base + 6] - ref[base + 6]) <= COST_REL * ref[base + 6]
+    assert abs(out[base + 16] - ref[base + 16]) <= 2 * 3
+    ctl_m = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, iterations=3, shared_focal=True,
+                            precision=tb._lib.TBA_PRECISION_MIXED)
+    out_m, rep_m = tb.solve_packed(device, ctl_m, s, i)
+    assert rep_m["engine"] == 1
+    assert abs(out_m[base + 6] - out[base + 6]) <= COST_REL * out[base + 6]
