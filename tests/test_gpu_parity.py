@@ -273,3 +273,36 @@ def test_beyond_the_shared_memory_limit_the_two_pass_engine_matches_the_oracle(d
     out_m, rep_m = tb.solve_packed(device, ctl_m, s, i)
     assert rep_m["engine"] == 1
     assert abs(out_m[base + 6] - out[base + 6]) <= COST_REL * out[base + 6]
+
+
+@pytest.mark.parametrize("name", ["all-fixed", "local", "all-fixed-shared", "local-shared", "global"])
+def test_fixed_camera_observations_still_optimize_points_and_focal(device, name):
+    # fixedJacobianCases / assertFixedJacobianCases (tests/typeshade/bundle-fixed-jacobian-cases.mjs:3-128).
+    import copy
+    local = name.startswith("local")
+    model = bundle_fixture(count=24, views=6, outlier=local)
+    shared = name.endswith("shared")
+    if shared:
+        model = {**model, "views": [{**v, "camera": {**v["camera"], "fx": v["camera"]["fx"] * 0.97,
+                                                     "fy": v["camera"]["fy"] * 0.97}} for v in model["views"]]}
+    variable_ids = None if name == "global" else ([v["id"] for v in model["views"][-2:]] if local else [])
+    variable = set(variable_ids if variable_ids is not None else [v["id"] for v in model["views"][1:]])
+    fixed_obs = sum(1 for p in model["landmarks"] for o in p["observations"] if o["viewId"] not in variable)
+    options = {"iterations": 3, "huberPx": 2, "refineSharedFocal": shared}
+    if variable_ids is not None:
+        options["variableViewIds"] = variable_ids
+    before = copy.deepcopy(model)
+    result = tb.bundle_adjust_gpu(device, model, options)
+    assert repr(model) == repr(before)
+    moved = {v["id"]: v for v in result["reconstruction"]["views"]}
+    for v in model["views"]:
+        if v["id"] not in variable:
+            assert np.array_equal(np.asarray(moved[v["id"]]["pose"]["R"]), np.asarray(v["pose"]["R"]))
+            assert np.array_equal(np.asarray(moved[v["id"]]["pose"]["t"]), np.asarray(v["pose"]["t"]))
+    d = result["diagnostics"]
+    assert d["acceptedSteps"] > 0 and d["finalCost"] < d["initialCost"] and fixed_obs > 0
+    ratio = result["reconstruction"]["views"][0]["camera"]["fx"] / model["views"][0]["camera"]["fx"]
+    if shared:
+        assert abs(ratio - 1) > 1e-6
+    else:
+        assert ratio == 1
