@@ -429,8 +429,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_scal = L.take<double>(size_t(tba::kScalarPartials) * max_task_blocks),
                o_cost = L.take<double>(4 * size_t(max_task_blocks)), o_ticket = L.take<uint32_t>(8),
                o_state = L.take<double>(tba::S_WORDS), o_out = L.take<double>(12 * size_t(C) + 3 * size_t(P) + 27),
-               o_keys = L.take<unsigned long long>(tba::CK_WORDS),
-               o_pc = L.take<uint2>(mixed && p.factored ? size_t(p.Mpad) : 0);
+               o_keys = L.take<unsigned long long>(tba::CK_WORDS);
   if (d->capacity < L.bytes) {
     if (d->arena) CUDA_TRY(cudaFree(d->arena));
     d->arena = nullptr;
@@ -473,8 +472,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.chunk_prod = D(o_cprod);
   p.F = p.factored && !mixed ? D(o_F) : nullptr;
   p.F32 = p.factored && mixed ? reinterpret_cast<float*>(a + o_F) : nullptr;
-  p.obs_pc = p.F32 ? reinterpret_cast<const uint2*>(a + o_pc) : nullptr;
-  p.bulk_cap = tba::product_bulk_cap(p);
   p.pw = D(o_pw);
   p.xw = D(o_xw);
   p.acc_part = D(o_acc);
@@ -585,7 +582,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   tail.factored = 0;
   tail.F = nullptr;
   tail.F32 = nullptr;
-  tail.bulk_cap = 0;
   tail.tol_inner = 0;  // the tail stops at the solve's own tolerance
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
     tba::launch_point_pass(p, s);
@@ -650,8 +646,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     CUDA_TRY(cudaStreamSynchronize(s));
     lm_active = d->pinned[tba::S_ACTIVE] != 0;
   }
-  if (p.bulk_cap && read_word(d, p.state, tba::S_DEVICE_ERROR) != 0)
-    throw Fail{TBA_ERROR_CUDA, "GPU BA: a staged round of the Schur product did not arrive"};
   tba::launch_pack(p, s);
   launches++;
   CUDA_TRY(cudaGetLastError());

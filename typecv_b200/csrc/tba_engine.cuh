@@ -49,7 +49,6 @@ enum StateWord : int {
   S_REFINE = 34,           // an FP64 refinement of the PCG solution is under way
   S_REFINED = 35,          // refinements that restarted the PCG (this solve)
   S_INNER_R0 = 36,         // residual^2 that the current inner PCG run is measured against
-  S_DEVICE_ERROR = 37,     // a bounded wait of a kernel ran out (the solve's result is not valid)
   S_WORDS = 64
 };
 
@@ -60,11 +59,6 @@ constexpr int kStagedThreads = 768;   // one block per SM, direction staged in s
 constexpr int kStagedSmemLimit = 227 * 1024 - 64;  // the dynamic share; the rest is static
 // Bytes of a product block's camera sums (6C values of `word` bytes), rounded to 16.
 __host__ __device__ inline size_t product_sums_bytes(uint32_t C, size_t word) { return (6 * size_t(C) * word + 15) / 16 * 16; }
-// Where the bulk-fed FP32 product's two stages start: after its FP32 sums and staged direction.
-__host__ __device__ inline size_t product_bulk_stage_offset(uint32_t C) {
-  return (product_sums_bytes(C, 4) + 24 * size_t(C) + 127) / 128 * 128;
-}
-constexpr int kBulkSmemLimit = kStagedSmemLimit - 512;  // its static words take the rest
 
 constexpr int kPointThreads = 256;  // threads of the task kernels
 constexpr int kCameraThreads = 128;
@@ -114,10 +108,6 @@ struct Params {
   uint32_t factored;   // 1: one-pass product over stored factors; 0: two-pass recompute
   uint32_t refine;     // 1: this launch evaluates the FP64 product S x of the refinement
   uint32_t prod_blocks;  // grid of the one-pass product
-  // The FP32-factor product fed by bulk copies (k_product_bulk): observations per staged round
-  // (0 when the kernel is not used) and each observation's (camera, point), padded to Mpad.
-  uint32_t bulk_cap;
-  const uint2* obs_pc;
   double* pw;          // 6C: the PCG direction of each camera in world axes (R^T omega, R^T v)
   double* xw;          // 6C: the PCG solution of each camera in world axes
   double* acc_part;    // prod_blocks x m: per-block camera sums of the one-pass product
@@ -166,9 +156,6 @@ uint32_t product_finish_blocks(const Params& p);
 // dynamic shared memory, the opt-in of the product kernels, and their blocks per SM.
 uint32_t product_max_unknowns();
 size_t product_smem_bytes(const Params& p);
-// Observations per staged round of the bulk-fed FP32 product for this problem, or 0 when its two
-// stages do not fit beside the camera sums and the staged direction.
-uint32_t product_bulk_cap(const Params& p);
 bool product_staged(const Params& p);
 int product_threads(const Params& p);
 cudaError_t configure_kernels();

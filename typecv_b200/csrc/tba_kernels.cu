@@ -32,10 +32,8 @@
 // shared-memory camera sums of k_product_f, whose FP64 atomic adds commute only up to rounding.
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <type_traits>
 
-#include "tba_bulk.cuh"
 #include "tba_engine.cuh"
 #include "tba_warp.cuh"
 
@@ -120,8 +118,6 @@ __global__ void k_initialize(Params P) {
 __global__ void k_setup(Params P) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < P.C) P.rlim[k] = radial_limit(P.cams[6 * size_t(k) + 4], P.cams[6 * size_t(k) + 5]);
-  if (P.obs_pc && k < P.Mpad)
-    const_cast<uint2*>(P.obs_pc)[k] = k < P.M ? uint2{P.obs_camera[k], P.obs_point[k]} : uint2{0u, 0u};
   if (k < P.M) {
     const uint32_t i = P.camera_obs[k];
     P.cm_point[k] = P.obs_point[i];
@@ -779,247 +775,6 @@ __global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STA
   if (SHARED && threadIdx.x == 0) out[m - 1] = focal_acc;
 }
 
-// The FP32-factor product fed by the copy engine.  The per-observation global loads of
-// k_product_f (12 factor words and two indices per lane) go through the L1 data pipe as whole
-// sectors and, with the shared-memory atomics and gathers, keep that pipe busy while DRAM runs at
-// a fraction of its peak.  Here a block's task range is cut into rounds of up to one task per warp
-// and `bulk_cap` observations; the block's producer thread copies the next round's factors (12
-// contiguous component segments) and (camera, point) pairs into one of two shared-memory stages
-// with cp.async.bulk while the warps work on the current round from the other stage.  The
-// arithmetic is k_product_f's, in the same order.  A task longer than a stage is read from global
-// memory in a round of its own.  Waits on a stage are bounded; a wait that runs out sets
-// S_DEVICE_ERROR and the block stops.
-constexpr int kBulkRoundWords = 4 + 33;  // task range, window start, direct flag, first observations
-
-template <bool SHARED>
-__global__ void __launch_bounds__(kStagedThreads, 1) k_product_bulk(Params P) {
-  extern __shared__ double4 product_smem[];
-  __shared__ double focal_acc;
-  __shared__ uint64_t bars[2];
-  __shared__ uint32_t rounds[2][kBulkRoundWords];
-  __shared__ uint32_t abort_flag;
-  if (P.state[S_CG_ACTIVE] == 0) return;
-  const uint32_t m = P.m, C = P.C;
-  float* acc = reinterpret_cast<float*>(product_smem);
-  float2* pws = reinterpret_cast<float2*>(reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, 4));
-  unsigned char* stages = reinterpret_cast<unsigned char*>(product_smem) + product_bulk_stage_offset(C);
-  const uint32_t cap = P.bulk_cap, S = cap + 8;  // stage stride in observations (a multiple of 8)
-  const uint32_t stage_bytes = 56 * S;
-  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) acc[j] = 0.f;
-  for (uint32_t j = threadIdx.x; j < 3 * C; j += blockDim.x) {
-    const uint32_t c = j / 3, k = j % 3;
-    pws[k * C + c] = float2{float(P.pw[6 * c + 2 * k]), float(P.pw[6 * c + 2 * k + 1])};
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  uint32_t tb, te;
-  block_tasks(P, tb, te);
-  uint32_t next_task = tb;  // warp 0: the first task not yet given a round
-  // Warp 0 forms the next round in stage s: one coalesced read of the candidate tasks' bounds
-  // (task_obs is nondecreasing, so the tasks that fit are a prefix), then lane 0 starts the copies
-  // or, for an empty round or one task longer than a stage (read from global memory), arrives
-  // without copies.
-  auto form = [&](int s) {
-    uint32_t* r = rounds[s];
-    const uint32_t t0 = next_task;
-    const uint32_t o0 = t0 < te ? P.task_obs[t0] : 0;
-    const uint32_t tl = t0 + 1 + uint32_t(lane);
-    const bool in = lane < nwarps && tl <= te;
-    const uint32_t oe = in ? P.task_obs[tl] : 0;
-    const bool take = in && (lane == 0 || oe - o0 <= cap);
-    const uint32_t count = __popc(__ballot_sync(kFull, take));
-    const uint32_t o1 = count ? __shfl_sync(kFull, oe, int(count) - 1) : o0;
-    if (uint32_t(lane) < count) r[5 + lane] = oe;
-    next_task = t0 + count;
-    const uint32_t direct = (count == 1 && o1 - o0 > cap) ? 1u : 0u;
-    const uint32_t a = o0 & ~3u, b = (o1 + 3) & ~3u;
-    if (lane == 0) {
-      r[0] = t0;
-      r[1] = t0 + count;
-      r[2] = a;
-      r[3] = direct;
-      r[4] = o0;
-    }
-    __syncwarp();
-    if (lane != 0) return;
-    const uint32_t bar = bulk_smem_addr(bars + s);
-    if (count == 0 || direct) {
-      bulk_arrive(bar);
-      return;
-    }
-    const uint32_t n = b - a;
-    unsigned char* st = stages + size_t(s) * stage_bytes;
-    bulk_expect(bar, 56 * n);
-    for (int k = 0; k < kFactors; k++)
-      bulk_load(bar, bulk_smem_addr(st + size_t(k) * 4 * S), P.F32 + size_t(k) * P.Mpad + a, 4 * n);
-    bulk_load(bar, bulk_smem_addr(st + size_t(kFactors) * 4 * S), P.obs_pc + a, 8 * n);
-  };
-  if (warp == 0) {
-    if (lane == 0) {
-      abort_flag = 0;
-      focal_acc = 0;
-      bulk_bar_init(bulk_smem_addr(bars));
-      bulk_bar_init(bulk_smem_addr(bars + 1));
-      bulk_bar_fence();
-    }
-    __syncwarp();
-    form(0);
-    form(1);
-  }
-  __syncthreads();
-  const double pf = SHARED ? P.p[m - 1] : 0.0;
-  double ef = 0;
-  for (uint32_t k = 0;; k++) {
-    const int s = int(k & 1);
-    if (!bulk_wait(bulk_smem_addr(bars + s), (k >> 1) & 1)) abort_flag = 1;
-    __syncthreads();
-    if (abort_flag) break;
-    const uint32_t* r = rounds[s];
-    const uint32_t t0 = r[0], t1 = r[1], a = r[2];
-    if (t0 == t1) break;
-    const bool direct = r[3] != 0;
-    const unsigned char* st = stages + size_t(s) * stage_bytes;
-    const float* sf = reinterpret_cast<const float*>(st);
-    const uint2* spc = reinterpret_cast<const uint2*>(st + size_t(kFactors) * 4 * S);
-    // Observation i of this round: its factors and its camera and point.
-    auto fetch = [&](uint32_t i, Factors<float>& f, uint32_t& c, uint32_t& pt) {
-      if (direct) {
-        load_factors(P.F32, P.Mpad, i, f);
-        c = P.obs_camera[i];
-        pt = P.obs_point[i];
-        return;
-      }
-      const uint32_t li = i - a;
-      f.q[0] = sf[li];
-      f.q[1] = sf[S + li];
-      f.q[2] = sf[2 * S + li];
-      f.ju[0] = sf[3 * S + li];
-      f.ju[1] = sf[4 * S + li];
-      f.ju[2] = sf[5 * S + li];
-      f.jv[0] = sf[6 * S + li];
-      f.jv[1] = sf[7 * S + li];
-      f.jv[2] = sf[8 * S + li];
-      f.w = sf[9 * S + li];
-      f.jf[0] = sf[10 * S + li];
-      f.jf[1] = sf[11 * S + li];
-      const uint2 v = spc[li];
-      c = v.x;
-      pt = v.y;
-    };
-    auto scatter = [&](const Factors<float>& f, uint32_t c, bool dir, float y0, float y1, float y2) {
-      const float gu = f.w * (f.ju[0] * y0 + f.ju[1] * y1 + f.ju[2] * y2);
-      const float gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
-      if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
-      const float h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      float* ac = acc + c;
-      atomicAdd(ac, -(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + C, -(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2 * C, -(f.q[0] * h1 - f.q[1] * h0));
-      if (!dir) {
-        atomicAdd(ac + 3 * C, -h0);
-        atomicAdd(ac + 4 * C, -h1);
-        atomicAdd(ac + 5 * C, -h2);
-      }
-    };
-    if (uint32_t(warp) < t1 - t0) {
-      const uint32_t o0 = r[4 + warp], n = r[5 + warp] - o0;
-      if (n <= uint32_t(kTaskObs)) {
-        const bool valid = uint32_t(lane) < n;
-        const uint32_t i = o0 + (valid ? lane : 0);
-        Factors<float> f;
-        uint32_t c, pt;
-        fetch(i, f, c, pt);
-        double vb[6], xw[6];
-        load6(P.pblk + 12 * size_t(pt), vb);
-        for (int q = 0; q < 3; q++) {
-          const float2 v = pws[q * C + c];
-          xw[2 * q] = double(v.x);
-          xw[2 * q + 1] = double(v.y);
-        }
-        const uint32_t p0 = __shfl_sync(kFull, pt, 0);
-        const int seg = valid ? int(pt - p0) : -1 - lane;
-        double sum[3] = {0, 0, 0};
-        if (valid) factor_wt(f, xw, pf, true, directional(P, pt), SHARED, sum);
-        const Runs runs = lane_runs(seg, lane);
-        run_scan(sum, runs);
-        const bool tail = valid && run_tail(runs, lane);
-        double y[3] = {0, 0, 0};
-        if (tail) {
-          y[0] = vb[0] * sum[0] + vb[1] * sum[1] + vb[2] * sum[2];
-          y[1] = vb[1] * sum[0] + vb[3] * sum[1] + vb[4] * sum[2];
-          y[2] = vb[2] * sum[0] + vb[4] * sum[1] + vb[5] * sum[2];
-        }
-        const unsigned tails = __ballot_sync(kFull, tail);
-        const int src = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
-        for (int q = 0; q < 3; q++) y[q] = __shfl_sync(kFull, y[q], src);
-        if (valid) scatter(f, c, directional(P, pt), float(y[0]), float(y[1]), float(y[2]));
-      } else {
-        // A point with more than 32 observations: rounds of 32, one warp-wide sum.
-        uint32_t p0;
-        {
-          Factors<float> f0;
-          uint32_t c0;
-          fetch(o0, f0, c0, p0);
-        }
-        const uint32_t nr = (n + kTaskObs - 1) / kTaskObs;
-        double sum[3] = {0, 0, 0};
-        for (uint32_t q = 0; q < nr; q++) {
-          const uint32_t kk = q * kTaskObs + lane;
-          if (kk < n) {
-            Factors<float> f;
-            uint32_t c, pt;
-            fetch(o0 + kk, f, c, pt);
-            double xw[6], u[3];
-            for (int z = 0; z < 3; z++) {
-              const float2 v = pws[z * C + c];
-              xw[2 * z] = double(v.x);
-              xw[2 * z + 1] = double(v.y);
-            }
-            factor_wt(f, xw, pf, true, directional(P, p0), SHARED, u);
-            sum[0] += u[0];
-            sum[1] += u[1];
-            sum[2] += u[2];
-          }
-        }
-        warp_allsum(sum);
-        double vb[6];
-        load6(P.pblk + 12 * size_t(p0), vb);
-        const float y0 = float(vb[0] * sum[0] + vb[1] * sum[1] + vb[2] * sum[2]);
-        const float y1 = float(vb[1] * sum[0] + vb[3] * sum[1] + vb[4] * sum[2]);
-        const float y2 = float(vb[2] * sum[0] + vb[4] * sum[1] + vb[5] * sum[2]);
-        for (uint32_t q = 0; q < nr; q++) {
-          const uint32_t kk = q * kTaskObs + lane;
-          if (kk >= n) continue;
-          Factors<float> f;
-          uint32_t c, pt;
-          fetch(o0 + kk, f, c, pt);
-          scatter(f, c, directional(P, p0), y0, y1, y2);
-        }
-      }
-    }
-    // Every warp is done with stage s (its reads ordered before the copy engine's next writes).
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (warp == 0) form(s);
-  }
-  if (abort_flag && threadIdx.x == 0) P.state[S_DEVICE_ERROR] = 1;
-  if (SHARED) {
-    for (int d = 16; d > 0; d >>= 1) ef += __shfl_xor_sync(kFull, ef, d);
-    if (lane == 0) atomicAdd(&focal_acc, -ef);
-  }
-  __syncthreads();
-  double* out = P.acc_part + size_t(blockIdx.x) * m;
-  for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
-    double av[6];
-    for (int j = 0; j < 6; j++) av[j] = double(acc[j * C + c]);
-    const double* R = P.poses + 12 * size_t(c);
-    for (int rr = 0; rr < 3; rr++) {
-      out[6 * c + rr] = R[3 * rr] * av[0] + R[3 * rr + 1] * av[1] + R[3 * rr + 2] * av[2];
-      out[6 * c + 3 + rr] = R[3 * rr] * av[3] + R[3 * rr + 1] * av[4] + R[3 * rr + 2] * av[5];
-    }
-  }
-  if (SHARED && threadIdx.x == 0) out[m - 1] = focal_acc;
-}
-
 // The column sums of the one-pass product's partial rows (fixed order), then the camera rows of
 // S p = U_c p_c + H_cf p_f + sum, their p . Sp share; the last block adds the focal row and forms
 // alpha (the reference's breakdown checks).
@@ -1620,20 +1375,6 @@ bool product_staged(const Params& p) {
   return product_sums_bytes(p.C, word) + 6 * size_t(p.C) * word <= size_t(kStagedSmemLimit);
 }
 
-uint32_t product_bulk_cap(const Params& p) {
-  if (!p.F32 || !p.factored || !product_staged(p)) return 0;
-  const size_t off = product_bulk_stage_offset(p.C);
-  if (off >= size_t(kBulkSmemLimit)) return 0;
-  const size_t per_stage = (size_t(kBulkSmemLimit) - off) / 2;
-  const size_t S = (per_stage / 56) & ~size_t(7);
-  if (S < 8 + 256) return 0;
-  return uint32_t(std::min<size_t>(S - 8, 1024));
-}
-
-static size_t product_bulk_smem_bytes(const Params& p) {
-  return product_bulk_stage_offset(p.C) + 2 * 56 * (size_t(p.bulk_cap) + 8);
-}
-
 size_t product_smem_bytes(const Params& p) {
   const size_t word = p.F32 ? sizeof(float) : sizeof(double);
   return product_sums_bytes(p.C, word) + (product_staged(p) ? 6 * size_t(p.C) * word : 0);
@@ -1655,11 +1396,6 @@ cudaError_t configure_kernels() {
   set(reinterpret_cast<const void*>(k_product_f<true, double, true>));
   set(reinterpret_cast<const void*>(k_product_f<false, float, true>));
   set(reinterpret_cast<const void*>(k_product_f<true, float, true>));
-  auto set_bulk = [&](const void* f) {
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kBulkSmemLimit);
-  };
-  set_bulk(reinterpret_cast<const void*>(k_product_bulk<false>));
-  set_bulk(reinterpret_cast<const void*>(k_product_bulk<true>));
   return e;
 }
 
@@ -1677,8 +1413,7 @@ int product_blocks_per_sm(const Params& p) {
 
 void launch_initialize(const Params& p, cudaStream_t s) {
   k_initialize<<<1, 1, 0, s>>>(p);
-  uint32_t n = p.M > p.C ? p.M : p.C;
-  if (p.obs_pc && p.Mpad > n) n = p.Mpad;
+  const uint32_t n = p.M > p.C ? p.M : p.C;
   k_setup<<<(n + 255) / 256, 256, 0, s>>>(p);
 }
 void launch_cost(const Params& p, cudaStream_t s) { k_cost<<<p.task_blocks, kPointThreads, 0, s>>>(p); }
@@ -1691,12 +1426,6 @@ void launch_camera_pass(const Params& p, cudaStream_t s) { k_camera_pass<<<p.nch
 void launch_camera_finish(const Params& p, cudaStream_t s) { k_camera_finish<<<(p.C + 127) / 128, 128, 0, s>>>(p); }
 void launch_pcg_init(const Params& p, cudaStream_t s) { k_pcg_init<<<1, 1024, 0, s>>>(p); }
 void launch_product(const Params& p, cudaStream_t s) {
-  if (p.factored && p.bulk_cap) {
-    const size_t smem = product_bulk_smem_bytes(p);
-    if (p.shared) k_product_bulk<true><<<p.prod_blocks, kStagedThreads, smem, s>>>(p);
-    else k_product_bulk<false><<<p.prod_blocks, kStagedThreads, smem, s>>>(p);
-    return;
-  }
   if (p.factored) {
     const size_t smem = product_smem_bytes(p);
     const int nt = product_threads(p);

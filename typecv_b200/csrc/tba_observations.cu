@@ -21,7 +21,6 @@
 
 #include <algorithm>
 
-#include "tba_bulk.cuh"
 #include "tba_math.cuh"
 #include "tba_observations.cuh"
 
@@ -195,6 +194,36 @@ constexpr int kIdIn = 34, kIdOut = 23;
 constexpr int kIdStages = 2;
 constexpr uint32_t kIdTileIn = kIdRows * kIdIn * 8, kIdTileOut = kIdRows * kIdOut * 8;
 constexpr size_t kIdSmem = size_t(kIdStages) * kIdTileIn + kIdTileOut + 64;
+constexpr uint32_t kIdWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void id_bar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+
+// One arrival that also announces `bytes` of transactions, then the bulk load that completes them.
+__device__ __forceinline__ void id_load_tile(uint32_t bar, uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool id_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t k = 0; k < kIdWaitLimit; k++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 __device__ __forceinline__ void inverse_depth_row(const double* m, double* o) {
   for (int k = 0; k < kIdOut; k++) o[k] = 0;
@@ -259,19 +288,15 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
   const uint32_t tiles = (count + kIdRows - 1) / kIdRows;
   const bool producer = threadIdx.x == 0;
   auto rows_of = [&](uint32_t tile) { return min(uint32_t(kIdRows), count - tile * kIdRows); };
-  auto load_tile = [](uint32_t bar, uint32_t dst, const double* src, uint32_t bytes) {
-    bulk_expect(bar, bytes);
-    bulk_load(bar, dst, src, bytes);
-  };
   if (producer) {
     abort_flag = 0;
-    for (int k = 0; k < kIdStages; k++) bulk_bar_init(bulk_smem_addr(bars + k));
-    bulk_bar_fence();
+    for (int k = 0; k < kIdStages; k++) id_bar_init(smem_addr(bars + k));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (int k = 0; k < kIdStages; k++) {
       const uint32_t tile = blockIdx.x + k * gridDim.x;
       if (tile < tiles)
-        load_tile(bulk_smem_addr(bars + k), bulk_smem_addr(stage + size_t(k) * kIdRows * kIdIn),
-                  in + size_t(tile) * kIdRows * kIdIn, rows_of(tile) * kIdIn * 8);
+        id_load_tile(smem_addr(bars + k), smem_addr(stage + size_t(k) * kIdRows * kIdIn),
+                     in + size_t(tile) * kIdRows * kIdIn, rows_of(tile) * kIdIn * 8);
     }
   }
   __syncthreads();
@@ -279,7 +304,7 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, k++) {
     const uint32_t s = k % kIdStages, parity = (k / kIdStages) & 1;
     const uint32_t n = rows_of(tile);
-    if (!bulk_wait(bulk_smem_addr(bars + s), parity)) {
+    if (!id_wait(smem_addr(bars + s), parity)) {
       atomicExch(error, 1u);
       abort_flag = 1;
     }
@@ -294,7 +319,7 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
     if (producer) {
       double* dst = out + size_t(tile) * kIdRows * kIdOut;
       const uint32_t bytes = n * kIdOut * 8, whole = bytes & ~15u;
-      asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(bulk_smem_addr(tile_out)),
+      asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(tile_out)),
                    "r"(whole)
                    : "memory");
       asm volatile("cp.async.bulk.commit_group;" ::: "memory");
@@ -302,8 +327,8 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
       // Refill this stage with the tile kIdStages turns ahead: every thread has finished reading it.
       const uint32_t next = tile + kIdStages * gridDim.x;
       if (next < tiles)
-        load_tile(bulk_smem_addr(bars + s), bulk_smem_addr(rows), in + size_t(next) * kIdRows * kIdIn,
-                  rows_of(next) * kIdIn * 8);
+        id_load_tile(smem_addr(bars + s), smem_addr(rows), in + size_t(next) * kIdRows * kIdIn,
+                     rows_of(next) * kIdIn * 8);
     }
   }
   if (producer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
