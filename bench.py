@@ -12,7 +12,8 @@ forms' final costs.  ``e2e`` is the same metric through the public call (``tba_b
 pinned host buffers: host checks, host-to-device copies, the solve and the device-to-host read inside
 the timed region).  The working set (~1.5 GB) is larger than the 126 MB L2, so no flush is needed.
 ``roofline`` describes the dominant kernel, the one-pass Schur product, from CUDA-event pairs the
-library records around every product launch.
+library records around every product launch of one more solve after the timed steps (the events
+would cost the timed solves about 3%).
 
 ``--config cfg3`` runs the batched local-window solve (512 arc windows, one persistent launch) and
 ``--config cfg4`` the adjoint of a 200-camera / 50k-point solve; ``--config invdepth`` the
@@ -309,15 +310,19 @@ def pinned_like(a, torch):
 
 
 def time_form(args, world, local, scene, precision, iterations):
-    """Warm-up and timed solves of one form; returns (reports, wall times, output, clocks)."""
+    """Warm-up and timed solves of one form, then one solve with CUDA events around every Schur
+    product (for the roofline: the events cost about 3% of the solve, so they stay out of the
+    timed steps); returns (reports of the timed steps, wall times, output, clocks, the
+    instrumented report)."""
     import torch
     import typecv_b200 as tb
     from typecv_b200 import _lib
     s_np, i_np = scene.packed()
     s_pin, i_pin = pinned_like(s_np, torch), pinned_like(i_np, torch)
-    ctl = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, iterations=iterations,
-                          shared_focal=True, huber=2.0, tolerance=1e-6, precision=precision,
-                          flags=_lib.TBA_FLAG_TIME_PRODUCTS)
+    kw = dict(anchor=0, scale_view=1, iterations=iterations, shared_focal=True, huber=2.0, tolerance=1e-6,
+              precision=precision)
+    ctl = tb.make_control(scene.C, scene.P, scene.M, **kw)
+    ctl_timed = tb.make_control(scene.C, scene.P, scene.M, **kw, flags=_lib.TBA_FLAG_TIME_PRODUCTS)
     out = torch.empty(12 * scene.C + 3 * scene.P + 27, dtype=torch.float64, pin_memory=True).numpy()
     dev = tb.ShadeDevice.open(local)
     try:
@@ -333,9 +338,11 @@ def time_form(args, world, local, scene, precision, iterations):
                 reports.append(rep)
             barrier(world)
         clk = clocks.summary()
+        result = out.copy()
+        _, instrumented = tb.solve_packed(dev, ctl_timed, s_pin, i_pin, out)
     finally:
         dev.close()
-    return reports, walls, out.copy(), clk
+    return reports, walls, result, clk, instrumented
 
 
 def time_resident(args, world, local, scene, precision, iterations):
@@ -418,14 +425,14 @@ def run_single(args, world, rank, local):
     results = {}
     for form in forms:
         prec = _lib.TBA_PRECISION_MIXED if form == "mixed" else _lib.TBA_PRECISION_FP64
-        reports, walls, out, clk = time_form(args, world, local, scene, prec, iterations)
-        results[form] = (reports, walls, out, clk, form_summary(world, scene, reports, walls, out))
+        reports, walls, out, clk, instrumented = time_form(args, world, local, scene, prec, iterations)
+        results[form] = (reports, walls, out, clk, form_summary(world, scene, reports, walls, out), instrumented)
     if args.config == "cfg2" and forms[0] == "mixed":
         results["resident"] = time_resident(args, world, local, scene, _lib.TBA_PRECISION_MIXED, iterations)
     if rank != 0:
         return
     head = forms[0]
-    reports, walls, out, clk, summ = results[head]
+    reports, walls, out, clk, summ, instrumented = results[head]
     line = {
         "metric": METRIC, "value": summ["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * summ["t_max"] / args.steps, "higher_is_better": True,
@@ -436,7 +443,7 @@ def run_single(args, world, rank, local):
         "final_cost": summ["final_cost"], "final_rmse_px": summ["final_rmse_px"],
         "e2e": {"value": summ["e2e"], "unit": UNIT, "h2d_bytes_per_step": int(reports[-1]["h2d_bytes"]),
                 "d2h_bytes_per_step": int(reports[-1]["d2h_bytes"])},
-        "roofline": roofline(scene, reports, head),
+        "roofline": roofline(scene, [instrumented], head),
         "clocks": clk,
         "gpu_launches": sum(r["kernel_launches"] for r in reports),
     }
@@ -445,10 +452,10 @@ def run_single(args, world, rank, local):
         line["mixed"] = {"refinements": summ["refinements"], "cg_iterations": summ["cg_iterations"],
                          "pcg_failures": int(out[base + 17])}
     if len(forms) == 2:
-        r64, _, _, clk64, s64 = results["fp64"]
+        r64, _, _, clk64, s64, inst64 = results["fp64"]
         line["fp64"] = {"value": s64["value"], "e2e": s64["e2e"], "pcg_iterations_per_s": s64["pcg_iterations_per_s"],
                         "final_cost": s64["final_cost"], "final_rmse_px": s64["final_rmse_px"],
-                        "roofline": roofline(scene, r64, "fp64"), "clocks": clk64,
+                        "roofline": roofline(scene, [inst64], "fp64"), "clocks": clk64,
                         "gpu_launches": sum(r["kernel_launches"] for r in r64)}
         out64 = results["fp64"][2]
         n = 12 * scene.C + 3 * scene.P
