@@ -25,6 +25,7 @@
 #include "tba_adjoint.cuh"
 #include "tba_engine.cuh"
 #include "tba_math.cuh"
+#include "tba_warp.cuh"
 
 namespace tba {
 namespace {
@@ -437,6 +438,119 @@ __global__ void __launch_bounds__(128) k_adj_prod_cameras(AdjParams A) {
   }
 }
 
+// The Schur product in one pass over the cross blocks W_i (18 words, read once instead of twice):
+// each warp task forms y_p = V_p^-1 sum_i W_i^T p_c for its points (one observation per lane, a
+// segmented scan per point) and scatters -W_i y_p into the block's camera sums in shared memory;
+// k_adj_columns adds the blocks' partial rows in a fixed order and U_c p_c.
+constexpr int kAdjProductThreads = 256;
+constexpr int kAdjTaskObs = 32;
+
+__device__ inline void adj_wt(const double* W, const double* pc, double u[3]) {
+  u[0] = u[1] = u[2] = 0;
+  for (int a = 0; a < 6; a++) {
+    u[0] += W[3 * a] * pc[a];
+    u[1] += W[3 * a + 1] * pc[a];
+    u[2] += W[3 * a + 2] * pc[a];
+  }
+}
+
+__device__ inline void adj_scatter(double* acc, uint32_t C, uint32_t c, const double* W, const double y[3]) {
+  for (int a = 0; a < 6; a++)
+    atomicAdd(acc + size_t(a) * C + c, -(W[3 * a] * y[0] + W[3 * a + 1] * y[1] + W[3 * a + 2] * y[2]));
+}
+
+__global__ void __launch_bounds__(kAdjProductThreads) k_adj_product(AdjParams A) {
+  extern __shared__ double adj_acc[];  // 6C, component-major: value a of camera c at a * C + c
+  if (A.state[A_ACTIVE] == 0) return;
+  const uint32_t C = A.C;
+  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) adj_acc[j] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t tb = uint32_t(uint64_t(A.ntasks) * blockIdx.x / gridDim.x);
+  const uint32_t te = uint32_t(uint64_t(A.ntasks) * (blockIdx.x + 1) / gridDim.x);
+  for (uint32_t t = tb + warp; t < te; t += nwarps) {
+    const uint32_t o0 = A.task_obs[t], n = A.task_obs[t + 1] - o0;
+    if (n <= uint32_t(kAdjTaskObs)) {
+      const bool valid = uint32_t(lane) < n;
+      const uint32_t i = o0 + (valid ? lane : 0);
+      const uint32_t c = A.obs_camera[i], pt = A.obs_point[i];
+      const bool act = valid && A.active[c] != 0;
+      double W[18], pc[6], vb[6];
+      const double2* w2 = reinterpret_cast<const double2*>(A.Hcp + 18 * size_t(i));
+      for (int k = 0; k < 9; k++) {
+        const double2 v = w2[k];
+        W[2 * k] = v.x;
+        W[2 * k + 1] = v.y;
+      }
+      load6(A.p + 6 * size_t(c), pc);
+      load6(A.Vinv + 6 * size_t(pt), vb);
+      const uint32_t p0 = __shfl_sync(kFull, pt, 0);
+      const int seg = valid ? int(pt - p0) : -1 - lane;
+      double u[3] = {0, 0, 0};
+      if (act) adj_wt(W, pc, u);
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(u, runs);
+      const bool tail = valid && run_tail(runs, lane);
+      double y[3] = {0, 0, 0};
+      if (tail) {
+        y[0] = vb[0] * u[0] + vb[1] * u[1] + vb[2] * u[2];
+        y[1] = vb[1] * u[0] + vb[3] * u[1] + vb[4] * u[2];
+        y[2] = vb[2] * u[0] + vb[4] * u[1] + vb[5] * u[2];
+      }
+      const unsigned tails = __ballot_sync(kFull, tail);
+      const int src = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
+      for (int k = 0; k < 3; k++) y[k] = __shfl_sync(kFull, y[k], src);
+      if (act) adj_scatter(adj_acc, C, c, W, y);
+      continue;
+    }
+    // A point with more than 32 observations: rounds of 32, one warp-wide sum.
+    const uint32_t p0 = A.obs_point[o0];
+    const uint32_t rounds = (n + kAdjTaskObs - 1) / kAdjTaskObs;
+    double u[3] = {0, 0, 0};
+    for (uint32_t r = 0; r < rounds; r++) {
+      const uint32_t k = r * kAdjTaskObs + lane;
+      if (k >= n) continue;
+      const uint32_t i = o0 + k, c = A.obs_camera[i];
+      if (A.active[c] == 0) continue;
+      double v[3];
+      adj_wt(A.Hcp + 18 * size_t(i), A.p + 6 * size_t(c), v);
+      u[0] += v[0];
+      u[1] += v[1];
+      u[2] += v[2];
+    }
+    warp_allsum(u);
+    double vb[6];
+    load6(A.Vinv + 6 * size_t(p0), vb);
+    const double y[3] = {vb[0] * u[0] + vb[1] * u[1] + vb[2] * u[2], vb[1] * u[0] + vb[3] * u[1] + vb[4] * u[2],
+                         vb[2] * u[0] + vb[4] * u[1] + vb[5] * u[2]};
+    for (uint32_t r = 0; r < rounds; r++) {
+      const uint32_t k = r * kAdjTaskObs + lane;
+      if (k >= n) continue;
+      const uint32_t i = o0 + k, c = A.obs_camera[i];
+      if (A.active[c] != 0) adj_scatter(adj_acc, C, c, A.Hcp + 18 * size_t(i), y);
+    }
+  }
+  __syncthreads();
+  double* out = A.part + size_t(blockIdx.x) * 6 * C;
+  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) out[j] = adj_acc[(j % 6) * C + j / 6];
+}
+
+// S p = U_c p_c + the blocks' partial rows, summed in block order.
+__global__ void __launch_bounds__(256) k_adj_columns(AdjParams A) {
+  if (A.state[A_ACTIVE] == 0) return;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= 6 * A.C) return;
+  const uint32_t c = j / 6, a = j % 6;
+  double s = 0;
+  if (A.active[c] != 0)
+    for (uint32_t b = 0; b < A.prod_blocks; b++) s += A.part[size_t(b) * 6 * A.C + j];
+  const double* U = A.U + 21 * size_t(c);
+  const double* pc = A.p + 6 * size_t(c);
+  double up = 0;
+  for (int k = 0; k < 6; k++) up += U[sym6(a, k)] * pc[k];
+  A.Sp[j] = up + s;
+}
+
 __global__ void __launch_bounds__(1024) k_adj_vec(AdjParams A) {
   __shared__ double red[64];
   double* st = A.state;
@@ -739,9 +853,20 @@ uint32_t adj_launch_pcg_init(const AdjParams& a, cudaStream_t s) {
   return 1;
 }
 
+uint32_t adj_one_pass_max_cameras() { return (227 * 1024 - 1024) / (6 * sizeof(double)); }
+
+cudaError_t adj_configure() {
+  return cudaFuncSetAttribute(k_adj_product, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
+}
+
 uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
-  k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
-  k_adj_prod_cameras<<<a.C, 128, 0, s>>>(a);
+  if (a.prod_blocks) {
+    k_adj_product<<<a.prod_blocks, kAdjProductThreads, 6 * sizeof(double) * a.C, s>>>(a);
+    k_adj_columns<<<(6 * a.C + 255) / 256, 256, 0, s>>>(a);
+  } else {
+    k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
+    k_adj_prod_cameras<<<a.C, 128, 0, s>>>(a);
+  }
   k_adj_vec<<<1, 1024, 0, s>>>(a);
   return 3;
 }

@@ -77,7 +77,18 @@ struct AdjParams {
   double* tpoints;  // 3P
   double mu;        // damping of the Newton steps (H + mu G); 0: exact Newton
   uint32_t rhs_mode;  // 0: Newton (-gradient), 1: adjoint (cot)
+  // The one-pass Schur product (when the camera sums fit a block's shared memory): warp tasks of
+  // whole points (at most 32 observations, or one longer point), their first observations, and the
+  // per-block partial camera rows.
+  const uint32_t* task_obs;  // ntasks + 1
+  uint32_t ntasks;
+  uint32_t prod_blocks;      // 0: the two-pass product
+  double* part;              // prod_blocks x 6C
 };
+
+// The largest camera count of the one-pass product (its camera sums in one block's shared memory).
+uint32_t adj_one_pass_max_cameras();
+cudaError_t adj_configure();  // the one-pass product's shared-memory limit
 
 uint32_t adj_launch_init(const AdjParams& a, cudaStream_t s);        // gauge origin and baseline
 uint32_t adj_launch_reset(const AdjParams& a, cudaStream_t s);       // zero the per-solve sums and flags

@@ -1044,6 +1044,14 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   A.normalize_scale = fixed == 1;
   A.huber = vc->huber;
   A.tol = vc->cg_tolerance;
+  // Warp tasks of the one-pass Schur product (whole points, at most 32 observations each).
+  const std::vector<uint32_t> tasks = build_tasks(index + 2 * size_t(M), P);
+  std::vector<uint32_t> task_obs(tasks.size());
+  for (size_t t = 0; t < tasks.size(); t++) task_obs[t] = index[2 * size_t(M) + tasks[t]];
+  A.ntasks = uint32_t(tasks.size() - 1);
+  A.prod_blocks = C <= tba::adj_one_pass_max_cameras()
+                      ? std::max<uint32_t>(1, std::min<uint32_t>(8 * uint32_t(d->sms), (A.ntasks + 7) / 8))
+                      : 0;
   Layout L;
   const size_t o_poses = L.take<double>(12 * size_t(C)), o_points = L.take<double>(3 * size_t(P)),
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
@@ -1057,7 +1065,8 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
                o_vec = L.take<double>(5 * 6 * size_t(C)), o_cot = L.take<double>(6 * size_t(C) + 3 * size_t(P)),
                o_gcot = L.take<double>(12 * size_t(C) + 3 * size_t(P)), o_ybar = L.take<double>(2 * size_t(M)),
                o_state = L.take<double>(tba::A_WORDS), o_tposes = L.take<double>(12 * size_t(C)),
-               o_tpoints = L.take<double>(3 * size_t(P));
+               o_tpoints = L.take<double>(3 * size_t(P)), o_tobs = L.take<uint32_t>(task_obs.size()),
+               o_part = L.take<double>(size_t(A.prod_blocks) * 6 * C);
   if (d->capacity < L.bytes) {
     if (d->arena) CUDA_TRY(cudaFree(d->arena));
     d->arena = nullptr;
@@ -1107,6 +1116,8 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   A.state = D(o_state);
   A.tposes = D(o_tposes);
   A.tpoints = D(o_tpoints);
+  A.task_obs = reinterpret_cast<const uint32_t*>(a + o_tobs);
+  A.part = D(o_part);
   A.mu = 0;
 
   cudaStream_t s = d->stream;
@@ -1120,6 +1131,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   up(const_cast<double*>(A.cams), scene + 12 * size_t(C) + 3 * size_t(P), 6 * sizeof(double) * C);
   up(const_cast<double*>(A.pixels), scene + 18 * size_t(C) + 3 * size_t(P), 2 * sizeof(double) * M);
   up(dindex, index, sizeof(uint32_t) * (3 * size_t(M) + P + 2 * size_t(C) + 2));
+  up(const_cast<uint32_t*>(A.task_obs), task_obs.data(), sizeof(uint32_t) * task_obs.size());
   uint32_t launches = 0;
   launches += tba::adj_launch_init(A, s);
   CUDA_TRY(cudaGetLastError());
@@ -1361,6 +1373,7 @@ tba_status tba_device_open(int ordinal, tba_device** out) {
     CUDA_TRY(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMallocHost(&d->pinned, 64 * sizeof(double)));
     CUDA_TRY(tba::configure_kernels());
+    CUDA_TRY(tba::adj_configure());
     CUDA_TRY(tba::batch_configure());
   } catch (const Fail& f) {
     g_open_error = f.message;
