@@ -22,6 +22,8 @@
 // d2q/(d omega_a dX_m) = e_a x R e_m are the second-order terms of q = exp(omega)(R X + t) + v.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "tba_adjoint.cuh"
 #include "tba_engine.cuh"
 #include "tba_math.cuh"
@@ -459,13 +461,18 @@ __device__ inline void adj_scatter(double* acc, uint32_t C, uint32_t c, const do
     atomicAdd(acc + size_t(a) * C + c, -(W[3 * a] * y[0] + W[3 * a + 1] * y[1] + W[3 * a + 2] * y[2]));
 }
 
+// With few cameras (PRIVATE) every warp keeps its own copy of the camera sums, so that the warps'
+// atomic adds do not contend for the same few addresses; the copies are summed at the end.
+template <bool PRIVATE>
 __global__ void __launch_bounds__(kAdjProductThreads) k_adj_product(AdjParams A) {
-  extern __shared__ double adj_acc[];  // 6C, component-major: value a of camera c at a * C + c
+  extern __shared__ double adj_smem[];  // PRIVATE: one 6C copy per warp, else one; component-major
   if (A.state[A_ACTIVE] == 0) return;
   const uint32_t C = A.C;
-  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) adj_acc[j] = 0;
-  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t copies = PRIVATE ? uint32_t(nwarps) : 1u;
+  for (uint32_t j = threadIdx.x; j < copies * 6 * C; j += blockDim.x) adj_smem[j] = 0;
+  __syncthreads();
+  double* adj_acc = adj_smem + (PRIVATE ? size_t(warp) * 6 * C : 0);
   const uint32_t tb = uint32_t(uint64_t(A.ntasks) * blockIdx.x / gridDim.x);
   const uint32_t te = uint32_t(uint64_t(A.ntasks) * (blockIdx.x + 1) / gridDim.x);
   for (uint32_t t = tb + warp; t < te; t += nwarps) {
@@ -532,7 +539,12 @@ __global__ void __launch_bounds__(kAdjProductThreads) k_adj_product(AdjParams A)
   }
   __syncthreads();
   double* out = A.part + size_t(blockIdx.x) * 6 * C;
-  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) out[j] = adj_acc[(j % 6) * C + j / 6];
+  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) {
+    const size_t at = size_t(j % 6) * C + j / 6;
+    double v = 0;
+    for (uint32_t w = 0; w < copies; w++) v += adj_smem[size_t(w) * 6 * C + at];
+    out[j] = v;
+  }
 }
 
 // S p = U_c p_c + the blocks' partial rows, summed in block order.
@@ -853,15 +865,33 @@ uint32_t adj_launch_pcg_init(const AdjParams& a, cudaStream_t s) {
   return 1;
 }
 
-uint32_t adj_one_pass_max_cameras() { return (227 * 1024 - 1024) / (6 * sizeof(double)); }
+constexpr size_t kAdjSmemLimit = 227 * 1024 - 1024;
+
+uint32_t adj_one_pass_max_cameras() { return uint32_t(kAdjSmemLimit / (6 * sizeof(double))); }
+
+// Per-warp copies of the camera sums when two blocks of them fit an SM.
+bool adj_private_sums(uint32_t C) {
+  return size_t(kAdjProductThreads / 32) * 6 * sizeof(double) * C <= kAdjSmemLimit / 2;
+}
+
+uint32_t adj_product_blocks_per_sm(uint32_t C) {
+  const size_t bytes = (adj_private_sums(C) ? size_t(kAdjProductThreads / 32) : 1) * 6 * sizeof(double) * C;
+  return uint32_t(std::max<size_t>(1, std::min<size_t>(8, (228 * 1024) / (bytes + 1024))));
+}
 
 cudaError_t adj_configure() {
-  return cudaFuncSetAttribute(k_adj_product, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
+  cudaError_t e = cudaFuncSetAttribute(k_adj_product<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAdjSmemLimit));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_adj_product<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAdjSmemLimit));
+  return e;
 }
 
 uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
   if (a.prod_blocks) {
-    k_adj_product<<<a.prod_blocks, kAdjProductThreads, 6 * sizeof(double) * a.C, s>>>(a);
+    const bool priv = adj_private_sums(a.C);
+    const size_t smem = (priv ? size_t(kAdjProductThreads / 32) : 1) * 6 * sizeof(double) * a.C;
+    if (priv) k_adj_product<true><<<a.prod_blocks, kAdjProductThreads, smem, s>>>(a);
+    else k_adj_product<false><<<a.prod_blocks, kAdjProductThreads, smem, s>>>(a);
     k_adj_columns<<<(6 * a.C + 255) / 256, 256, 0, s>>>(a);
   } else {
     k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);

@@ -88,6 +88,8 @@ struct AdjParams {
 
 // The largest camera count of the one-pass product (its camera sums in one block's shared memory).
 uint32_t adj_one_pass_max_cameras();
+// Blocks per SM of the one-pass product for C cameras (its shared-memory camera sums).
+uint32_t adj_product_blocks_per_sm(uint32_t C);
 cudaError_t adj_configure();  // the one-pass product's shared-memory limit
 
 uint32_t adj_launch_init(const AdjParams& a, cudaStream_t s);        // gauge origin and baseline

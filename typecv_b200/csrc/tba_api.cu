@@ -1050,7 +1050,8 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
   for (size_t t = 0; t < tasks.size(); t++) task_obs[t] = index[2 * size_t(M) + tasks[t]];
   A.ntasks = uint32_t(tasks.size() - 1);
   A.prod_blocks = C <= tba::adj_one_pass_max_cameras()
-                      ? std::max<uint32_t>(1, std::min<uint32_t>(8 * uint32_t(d->sms), (A.ntasks + 7) / 8))
+                      ? std::max<uint32_t>(1, std::min<uint32_t>(tba::adj_product_blocks_per_sm(C) * uint32_t(d->sms),
+                                                                 (A.ntasks + 7) / 8))
                       : 0;
   Layout L;
   const size_t o_poses = L.take<double>(12 * size_t(C)), o_points = L.take<double>(3 * size_t(P)),
