@@ -547,20 +547,28 @@ __global__ void __launch_bounds__(kAdjProductThreads) k_adj_product(AdjParams A)
   }
 }
 
-// S p = U_c p_c + the blocks' partial rows, summed in block order.
+// S p = U_c p_c + the blocks' partial rows: 32 rows per block, each of its 8 warps summing every
+// 8th block's partial rows (coalesced), then the 8 sums in a fixed order.
 __global__ void __launch_bounds__(256) k_adj_columns(AdjParams A) {
+  __shared__ double part[8][33];
   if (A.state[A_ACTIVE] == 0) return;
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= 6 * A.C) return;
-  const uint32_t c = j / 6, a = j % 6;
+  const uint32_t n = 6 * A.C;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t j = blockIdx.x * 32 + lane;
   double s = 0;
-  if (A.active[c] != 0)
-    for (uint32_t b = 0; b < A.prod_blocks; b++) s += A.part[size_t(b) * 6 * A.C + j];
+  if (j < n)
+    for (uint32_t b = warp; b < A.prod_blocks; b += 8) s += A.part[size_t(b) * n + j];
+  part[warp][lane] = s;
+  __syncthreads();
+  if (warp != 0 || j >= n) return;
+  double sum = 0;
+  for (int w = 0; w < 8; w++) sum += part[w][lane];
+  const uint32_t c = j / 6, a = j % 6;
   const double* U = A.U + 21 * size_t(c);
   const double* pc = A.p + 6 * size_t(c);
   double up = 0;
   for (int k = 0; k < 6; k++) up += U[sym6(a, k)] * pc[k];
-  A.Sp[j] = up + s;
+  A.Sp[j] = up + (A.active[c] != 0 ? sum : 0.0);
 }
 
 __global__ void __launch_bounds__(1024) k_adj_vec(AdjParams A) {
@@ -892,7 +900,7 @@ uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
     const size_t smem = (priv ? size_t(kAdjProductThreads / 32) : 1) * 6 * sizeof(double) * a.C;
     if (priv) k_adj_product<true><<<a.prod_blocks, kAdjProductThreads, smem, s>>>(a);
     else k_adj_product<false><<<a.prod_blocks, kAdjProductThreads, smem, s>>>(a);
-    k_adj_columns<<<(6 * a.C + 255) / 256, 256, 0, s>>>(a);
+    k_adj_columns<<<(6 * a.C + 31) / 32, 256, 0, s>>>(a);
   } else {
     k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
     k_adj_prod_cameras<<<a.C, 128, 0, s>>>(a);
