@@ -7,9 +7,8 @@ Follows src/geometry/inverse-depth.ts: `initializeInverseDepth` (:19-35) and `in
 compares its device linearisation with (tests/typeshade/inverse-depth-cases.mjs:126-165).
 
 `bundle_adjust_inverse_depth` is the reference's CPU `bundleAdjustInverseDepth`
-(src/sfm/depth/inverse-depth-bundle.ts:717-729): the same host steps as the device operator (the
-reference shares `inverseDepthBundleSteps` between its two arms, so the steps here are the
-package's), answered with this file's CPU linearisation.  `fit_inverse_depth` restates
+(src/sfm/depth/inverse-depth-bundle.ts:717-729): the host steps restated loop for loop
+(oracle/inverse_depth_steps.py), answered with this file's CPU linearisation.  `fit_inverse_depth` restates
 `fitInverseDepth` (src/geometry/inverse-depth.ts:184-249) with `solveSystem`
 (src/geometry/numerics.ts:71-100), which the reference's bundle tests use as the fixed-pose baseline.
 """
@@ -163,7 +162,9 @@ def linearize_job(job):
 
 
 def bundle_adjust_inverse_depth(inp, constraints=(), options=None):
-    from typecv_b200.inverse_depth_bundle import drive, inverse_depth_bundle_steps
+    """The reference's CPU `bundleAdjustInverseDepth` (inverse-depth-bundle.ts:720-729): the restated
+    host steps (oracle/inverse_depth_steps.py) answered with this file's CPU linearisation."""
+    from oracle.inverse_depth_steps import drive, inverse_depth_bundle_steps
     return drive(inverse_depth_bundle_steps(inp, constraints, options), linearize_job)
 
 

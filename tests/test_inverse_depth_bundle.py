@@ -1,5 +1,7 @@
-"""Joint inverse-depth bundle adjustment: the host steps (typecv_b200/inverse_depth_bundle.py) driven by
-the oracle's CPU linearisation, i.e. the reference's CPU `bundleAdjustInverseDepth`.
+"""Joint inverse-depth bundle adjustment on the CPU: the restated host steps
+(oracle/inverse_depth_steps.py) driven by the oracle's CPU linearisation, i.e. the reference's CPU
+`bundleAdjustInverseDepth`, and the package's own host steps (typecv_b200/inverse_depth_bundle.py)
+held to it.
 
 Restates tests/inverse-depth-bundle.test.ts:9-139 and tests/inverse-depth-sparse.test.ts:7-164 on the
 same fixtures (tests/scene.ts restated in reference_cases.scene), plus the control checks of
@@ -13,7 +15,7 @@ import pytest
 
 from oracle import inverse_depth as oid
 from reference_cases import scene, seeded_random, update_pose
-from typecv_b200.bundle import RangeError
+RangeError = ValueError  # both the package's and the oracle's RangeError derive from it
 from typecv_b200.inverse_depth import camera_center
 
 BA = oid.bundle_adjust_inverse_depth
