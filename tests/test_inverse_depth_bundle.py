@@ -212,3 +212,158 @@ def test_controls_are_checked():
                                          reconstruction["views"][2]]}
     with pytest.raises(RangeError, match="pure rotation"):
         BA(moved, [], {})
+
+
+# ---- the package's array-wise host steps held to the oracle's loop restatement ----------------------
+
+def product_ba(inp, constraints=(), options=None):
+    """typecv_b200's host steps answered by the oracle's C++ linearisation (no device)."""
+    from typecv_b200 import inverse_depth_bundle as IDB
+    return IDB.drive(IDB.inverse_depth_bundle_steps(inp, constraints, options),
+                     lambda job: oid.linearize_rows(job["rows"]))
+
+
+EXACT = ("acceptedSteps", "observations", "cameraParameters", "linearSolver", "schurEntries", "factorEntries",
+         "cameraCovarianceEntries", "pointCrossEntries", "denseEquivalentCrossEntries", "inputObservations",
+         "deferredTrackIds")
+
+
+def assert_same_solve(got, want, cost=1e-9, state=1e-8, covariance=1e-7, converged=False):
+    """Same diagnostics, costs, poses, points and covariances.  Once the solve has converged a
+    candidate's cost differs from the current one by rounding only, and which of those steps are
+    taken is not part of the comparison (``converged``)."""
+    dg, dw = got["diagnostics"], want["diagnostics"]
+    for key in EXACT:
+        if key == "acceptedSteps" and converged:
+            continue
+        assert dg[key] == dw[key], (key, dg[key], dw[key])
+    for key in ("initialCost", "finalCost"):
+        assert abs(dg[key] - dw[key]) <= cost * max(1.0, abs(dw[key])), (key, dg[key], dw[key])
+    assert got["uncertainty"] == want["uncertainty"]
+    for a, b in zip(got["reconstruction"]["views"], want["reconstruction"]["views"]):
+        assert a["id"] == b["id"]
+        assert np.max(np.abs(np.asarray(a["pose"]["R"]) - np.asarray(b["pose"]["R"]))) < state
+        assert np.max(np.abs(np.asarray(a["pose"]["t"]) - np.asarray(b["pose"]["t"]))) < state
+        assert abs(a["camera"]["fx"] / b["camera"]["fx"] - 1) < state
+    assert [p["trackId"] for p in got["reconstruction"]["landmarks"]] == \
+        [p["trackId"] for p in want["reconstruction"]["landmarks"]]
+    for a, b in zip(got["reconstruction"]["landmarks"], want["reconstruction"]["landmarks"]):
+        assert np.max(np.abs(np.asarray(a["xyz"]) - np.asarray(b["xyz"]))) < state * max(1.0, np.max(np.abs(b["xyz"])))
+    assert len(got["estimates"]) == len(want["estimates"])
+    for a, b in zip(got["estimates"], want["estimates"]):
+        assert a["trackId"] == b["trackId"] and a.get("informationDeferred") == b.get("informationDeferred")
+        assert np.max(np.abs(np.asarray(a["point"]["parameters"]) - np.asarray(b["point"]["parameters"]))) < state
+        assert np.max(np.abs(np.asarray(a["point"]["reference"]["t"]) - np.asarray(b["point"]["reference"]["t"]))) < state
+        for key in ("covariance", "bearingCovariance"):
+            assert (a.get(key) is None) == (b.get(key) is None), key
+            if b.get(key) is not None:
+                ca, cb = np.asarray(a[key]), np.asarray(b[key])
+                scale = np.sqrt(np.outer(np.abs(np.diag(cb.reshape(int(math.isqrt(cb.size)), -1))),
+                                         np.abs(np.diag(cb.reshape(int(math.isqrt(cb.size)), -1))))).ravel()
+                assert np.max(np.abs(ca - cb) / scale) < covariance, key
+
+
+def perturbed_scene(count=30, views=4, seed_noise=0.1):
+    reconstruction, rng = scene(count=count, views=views, noise=seed_noise)
+    out = []
+    for i, v in enumerate(reconstruction["views"]):
+        if i == 0:
+            out.append(v)
+            continue
+        delta = [(rng() - 0.5) * s for s in (0.002, 0.002, 0.002, 0.01, 0.01, 0.01)]
+        R, t = update_pose(list(v["pose"]["R"]), list(v["pose"]["t"]), delta)
+        out.append({**v, "pose": {"R": np.array(R), "t": np.array(t)}})
+    landmarks = [{**p, "xyz": np.array([x + (rng() - 0.5) * 0.03 for x in p["xyz"]])} for p in reconstruction["landmarks"]]
+    return {"views": out, "landmarks": landmarks}
+
+
+@pytest.mark.parametrize("options", [
+    {"iterations": 4},
+    {"iterations": 6, "refineSharedFocal": True},
+    {"iterations": 4, "solver": "sparse"},
+    {"iterations": 4, "solver": "sparse", "refineSharedFocal": True, "huberPx": 0.05},
+    {"iterations": 3, "variableViewIds": [30, 40]},
+    {"iterations": 0, "pixelNoiseStdDevPx": 2},
+])
+def test_package_steps_match_the_oracle_steps(options):
+    inp = perturbed_scene()
+    assert_same_solve(product_ba(inp, [], options), BA(inp, [], options))
+
+
+def test_package_steps_match_past_convergence():
+    inp = perturbed_scene()
+    got, want = product_ba(inp, [], {"iterations": 12}), BA(inp, [], {"iterations": 12})
+    assert got["diagnostics"]["finalCost"] < got["diagnostics"]["initialCost"] * 1e-2
+    assert_same_solve(got, want, converged=True)
+
+
+def test_package_steps_match_on_a_shared_focal_error_and_focal_groups():
+    reconstruction, _ = scene(count=30, views=5, noise=0)
+    inp = {**reconstruction, "views": [{**v, "camera": {**v["camera"], "fx": v["camera"]["fx"] * 0.9,
+                                                          "fy": v["camera"]["fy"] * 0.9}} for v in reconstruction["views"]]}
+    options = {"iterations": 30, "refineSharedFocal": True}
+    assert_same_solve(product_ba(inp, [], options), BA(inp, [], options), cost=1e-7, converged=True)
+    groups = {"iterations": 5, "refineSharedFocal": True, "focalGroups": {v["id"]: v["id"] % 2 for v in inp["views"]}}
+    assert_same_solve(product_ba(inp, [], groups), BA(inp, [], groups))
+
+
+@pytest.mark.parametrize("solver", ["dense", "sparse"])
+def test_package_steps_match_with_a_deferred_track(solver):
+    reconstruction, _ = scene(count=30, views=4, noise=0)
+    base = reconstruction["views"][0]
+    views = reconstruction["views"] + [{**base, "id": 100}]
+    good = [{**p, "observations": p["observations"] + [
+        {"viewId": 100, "featureId": p["trackId"], "pixel": project_point(base["camera"], base["pose"], p["xyz"])}]}
+        for p in reconstruction["landmarks"]]
+    xyz = np.array([0.2, 0.1, 8.0])
+    pixel = project_point(base["camera"], base["pose"], xyz)
+    bad = {"trackId": 1000, "xyz": xyz, "observations": [{"viewId": base["id"], "featureId": 1000, "pixel": pixel},
+                                                         {"viewId": 100, "featureId": 1000, "pixel": pixel}]}
+    inp = {"views": views, "landmarks": good + [bad]}
+    got = product_ba(inp, [], {"solver": solver, "iterations": 2})
+    assert got["diagnostics"]["deferredTrackIds"] == [1000]
+    assert_same_solve(got, BA(inp, [], {"solver": solver, "iterations": 2}))
+
+
+def test_package_steps_match_with_constraints():
+    """Bearing-only and inverse-depth constraint tracks beside the landmarks (the 2 x 2 blocks and
+    the constraint checks of inverse-depth-bundle.ts:264-303)."""
+    inp = perturbed_scene(count=20)
+    views = inp["views"]
+    rng = seeded_random(77)
+    constraints = []
+    for k in range(6):
+        X = np.array([(rng() - 0.5) * 2, (rng() - 0.5) * 1.5, 6 + 2 * rng()])
+        obs = [{"viewId": v["id"], "featureId": 5000 + k, "pixel": project_point(v["camera"], v["pose"], X)}
+               for v in views[:3 if k % 2 else 4]]
+        ref = views[0]["pose"]
+        q = oid.transform_point(ref, X)
+        direction = k % 2 == 0
+        constraints.append({"trackId": 9000 + k, "observations": obs, "directionOnly": direction,
+                            "point": {"reference": {"R": ref["R"], "t": ref["t"]},
+                                      "parameters": [q[0] / q[2] + 0.001, q[1] / q[2] - 0.002,
+                                                     0.0 if direction else 1 / q[2] * 1.05]}})
+    for options in ({"iterations": 5}, {"iterations": 3, "solver": "sparse", "refineSharedFocal": True}):
+        got = product_ba(inp, constraints, options)
+        assert_same_solve(got, BA(inp, constraints, options))
+        assert all(e.get("bearingCovariance") is not None for e in got["estimates"][-6:])
+        assert all(e.get("covariance") is None for e in got["estimates"][-6::2])
+    with pytest.raises(RangeError, match="Bearing-only"):
+        product_ba(inp, [{**constraints[0], "point": {**constraints[0]["point"], "parameters": [0, 0, 1]}}])
+    with pytest.raises(RangeError, match="Multiply owned"):
+        product_ba(inp, [{**constraints[1], "observations": [inp["landmarks"][0]["observations"][0],
+                                                              *constraints[1]["observations"][1:]]}])
+
+
+def test_package_steps_match_on_the_long_camera_graph():
+    inp = long_scene(40)
+    got = product_ba(inp, [], {"iterations": 2})
+    assert got["diagnostics"]["linearSolver"] == "sparse"
+    assert_same_solve(got, BA(inp, [], {"iterations": 2}))
+    for options in ({"iterations": 0, "maxSchurEntries": 10}, {"iterations": 0, "solver": "sparse", "maxFactorEntries": 10},
+                    {"iterations": 0, "solver": "sparse", "maxFactorEntries": 2000}):
+        with pytest.raises(RangeError) as want:
+            BA(inp, [], options)
+        with pytest.raises(RangeError) as have:
+            product_ba(inp, [], options)
+        assert str(have.value) == str(want.value)

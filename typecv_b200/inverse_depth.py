@@ -116,6 +116,30 @@ def linearize_batches(device: ShadeDevice, job: dict, requested: int | None = No
     return {"rows": rows, "batches": batches, "batchSize": batch, "reports": reports}
 
 
+def linearize_rows(device: ShadeDevice, rows: np.ndarray, requested: int | None = None) -> dict[str, Any]:
+    """The same batching on rows already packed (n x 34): {"out": n x 23, batches, batchSize, reports}."""
+    if requested is not None and (isinstance(requested, bool) or not isinstance(requested, int) or requested < 1):
+        raise RangeError("Invalid inverse-depth measurement batch size")
+    rows = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 34)
+    count = len(rows)
+    if not count:
+        return {"out": np.zeros((0, 23)), "batches": 0, "batchSize": 0, "reports": []}
+    available = device.working_bytes if device.working_bytes is not None else 1 << 62
+    batch = min(count, requested if requested is not None else count, available // (8 * WORDS_PER_MEASUREMENT),
+                MAX_KERNEL_ELEMENTS)
+    if not batch >= 1:
+        raise RangeError("Inverse-depth measurement budget cannot fit one observation")
+    out = np.empty((count, 23))
+    reports, batches = [], 0
+    for first in range(0, count, batch):
+        n = min(batch, count - first)
+        o, rep = _linearize(device, rows[first:first + n].ravel(), n)
+        out[first:first + n] = o[:23 * n].reshape(n, 23)
+        reports.append(rep)
+        batches += 1
+    return {"out": out, "batches": batches, "batchSize": batch, "reports": reports}
+
+
 def linearize_inverse_depth_gpu(device: ShadeDevice, job: dict, batch_size: int | None = None):
     """linearizeInverseDepthGpu (inverse-depth.ts:108-114): one linearisation or None per measurement,
     in order."""
