@@ -684,6 +684,7 @@ def run_inverse_depth(args, world, rank, local):
                 reps.append(call())
                 walls.append(time.perf_counter() - t0)
             barrier(world)
+        joint = joint_inverse_depth(dev, args) if rank == 0 else None
     finally:
         dev.close()
     kernel_s = max_over_ranks(world, sum(r["evaluate_ms"] for r in reps) / 1000)
@@ -720,8 +721,37 @@ def run_inverse_depth(args, world, rank, local):
                          "note": f"k_linearize_inverse_depth, 456 algorithmic bytes per measurement; peak of {kind}"},
             "parity": {"rows_checked": M, "flags_equal": flags_equal, "max_rel_vs_oracle": worst,
                        "invalid_rows": invalid},
-            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": sum(r["kernel_launches"] for r in reps)}
+            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": sum(r["kernel_launches"] for r in reps),
+            "joint": joint}
     print(json.dumps(line), flush=True)
+
+
+def joint_inverse_depth(dev, args, iterations=4):
+    """The joint inverse-depth bundle adjustment (bundleAdjustInverseDepthGpu) on the seeded
+    120-view corridor: wall time of the call (device linearisations and projections, host FP64
+    steps), its device time and launches; beside it, unless --no-cpu-baseline, the oracle's loop
+    restatement of the reference's CPU bundleAdjustInverseDepth on the same input."""
+    from typecv_b200 import synthetic as S
+    from typecv_b200.inverse_depth_bundle import bundle_adjust_inverse_depth_gpu
+    inp = S.inverse_depth_corridor()
+    bundle_adjust_inverse_depth_gpu(dev, inp, [], {"iterations": 1})
+    t0 = time.perf_counter()
+    got = bundle_adjust_inverse_depth_gpu(dev, inp, [], {"iterations": iterations})
+    wall = time.perf_counter() - t0
+    d = got["diagnostics"]
+    out = {"workload": "inverse_depth_corridor: 120 views, 1404 tracks of 4 views, 5616 measurements, "
+                       f"{iterations} LM iterations", "ms": 1000 * wall, "device_ms": d["deviceMs"],
+           "gpu_launches": d["kernelLaunches"], "camera_parameters": d["cameraParameters"],
+           "linear_solver": d["linearSolver"], "initial_cost": d["initialCost"], "final_cost": d["finalCost"],
+           "accepted_steps": d["acceptedSteps"]}
+    if not args.no_cpu_baseline:
+        from oracle import inverse_depth as oid
+        t0 = time.perf_counter()
+        want = oid.bundle_adjust_inverse_depth(inp, [], {"iterations": iterations})
+        out["cpu_reference_ms"] = 1000 * (time.perf_counter() - t0)
+        out["final_cost_rel_diff_vs_cpu"] = abs(d["finalCost"] - want["diagnostics"]["finalCost"]) / \
+            want["diagnostics"]["finalCost"]
+    return out
 
 
 def observation_request(scene, limit=0.05, noise=1.0, max_error=3.0):

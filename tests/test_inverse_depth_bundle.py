@@ -367,3 +367,12 @@ def test_package_steps_match_on_the_long_camera_graph():
         with pytest.raises(RangeError) as have:
             product_ba(inp, [], options)
         assert str(have.value) == str(want.value)
+
+
+def test_package_steps_match_on_the_noisy_corridor():
+    """The seeded corridor of the joint inverse-depth benchmark (noisy pixels, perturbed start)."""
+    from typecv_b200.synthetic import inverse_depth_corridor
+    inp = inverse_depth_corridor(views=24)
+    got, want = product_ba(inp, [], {"iterations": 3}), BA(inp, [], {"iterations": 3})
+    assert got["diagnostics"]["finalCost"] < got["diagnostics"]["initialCost"] * 0.1
+    assert_same_solve(got, want)

@@ -17,6 +17,9 @@ camera record (fx, fy, cx, cy, k1, k2; src/contracts/camera-record.ts:12-38).
 * ``inverse_depth_rows`` inverse-depth measurements packed as the 34-word rows of
                     ``tba_linearize_inverse_depth``: points anchored in a ring camera, each seen by
                     one of the next cameras of the ring.
+* ``inverse_depth_corridor`` a reconstruction (views and landmarks as records) for the joint
+                    inverse-depth bundle adjustment: translated views along a corridor, each run of
+                    consecutive views seeing points of its own.
 
 Every scene then gets Gaussian pixel noise, uniform in-image outliers and a perturbed
 initialisation (rotation by an axis-angle of fixed size, translation by a fraction of its norm,
@@ -343,3 +346,38 @@ def inverse_depth_rows(seed=5, measurements=4 << 20, cameras=512, radius=5.0, cu
     rows[:, 33] = limit[obs]
     return rows
 
+
+
+def inverse_depth_corridor(seed=11, views=120, window=4, points=12, noise_px=0.2, pose_noise=0.004,
+                           point_noise=0.02) -> dict:
+    """{"views", "landmarks"} records: `views` cameras with identity rotation whose centres follow
+    a corridor (0.3 apart along x, small sinusoidal y and z), the camera of the inverse-depth
+    fixtures (fx 800, fy 760, cx 320, cy 240, k1 -0.03); every run of `window` consecutive views
+    sees `points` points of its own, 5-8 in front.  Pixels are exact projections plus Gaussian
+    noise; the views after the first and the points start perturbed."""
+    rng = np.random.default_rng(seed)
+    camera = {"fx": 800.0, "fy": 760.0, "cx": 320.0, "cy": 240.0, "k1": -0.03}
+    i = np.arange(views)
+    centres = np.stack([0.3 * i, 0.04 * np.sin(i), 0.02 * np.sin(0.2 * i)], axis=1)
+    out_views = []
+    for k in range(views):
+        t = -centres[k]
+        if k:
+            t = t + rng.normal(0, pose_noise, 3)
+        out_views.append({"id": k, "camera": dict(camera), "pose": {"R": np.eye(3).ravel(), "t": t}})
+    landmarks = []
+    for start in range(views - window + 1):
+        lo, hi = centres[start, 0], centres[start + window - 1, 0]
+        X = np.stack([rng.uniform(lo - 1, hi + 1, points), rng.uniform(-1, 1, points), rng.uniform(5, 8, points)],
+                     axis=1)
+        for j in range(points):
+            track = start * points + j
+            q = X[j][None, :] - centres[start:start + window]
+            x, y = q[:, 0] / q[:, 2], q[:, 1] / q[:, 2]
+            d = 1 + camera["k1"] * (x * x + y * y)
+            u = camera["fx"] * x * d + camera["cx"] + rng.normal(0, noise_px, window)
+            v = camera["fy"] * y * d + camera["cy"] + rng.normal(0, noise_px, window)
+            landmarks.append({"trackId": track, "xyz": X[j] + rng.normal(0, point_noise, 3),
+                              "observations": [{"viewId": start + w, "featureId": track, "pixel": [float(u[w]), float(v[w])]}
+                                               for w in range(window)]})
+    return {"views": out_views, "landmarks": landmarks}
