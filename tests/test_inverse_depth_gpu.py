@@ -145,3 +145,20 @@ def test_large_sparse_joint_solve_in_tail_batches(device):
     assert d["cameraParameters"] > 96 and d["linearSolver"] == "sparse" and gpu["uncertainty"]["poses"] == "joint"
     assert d["measurementBatches"] == 16
     assert abs(d["finalCost"] - cpu["diagnostics"]["finalCost"]) <= 1e-9 * max(1.0, cpu["diagnostics"]["finalCost"])
+
+
+def test_sliced_call_matches_the_oracle(device):
+    """A call of more than 262,144 rows runs as slices of whole 128-row tiles whose downloads overlap
+    the next slices' uploads: 600,001 rows make three launches, the last slice ragged, and every row
+    equals the C++ CPU linearisation (flags equal, values within 1e-8)."""
+    from typecv_b200.synthetic import inverse_depth_rows
+    rows = inverse_depth_rows(seed=9, measurements=600_001)
+    out = ID.linearize_rows(device, rows)
+    assert out["batches"] == 1 and out["reports"][0]["kernel_launches"] == 3
+    want = oid.linearize_rows(rows)
+    assert np.array_equal(out["out"][:, 0], want[:, 0])
+    ok = want[:, 0] == 1
+    assert ok.sum() > 500_000
+    assert np.max(np.abs(out["out"][ok] - want[ok]) / np.maximum(1, np.abs(want[ok]))) < 1e-8
+    again = ID.linearize_rows(device, rows, 262_145)
+    assert again["batches"] == 3 and np.array_equal(again["out"], out["out"])

@@ -33,6 +33,7 @@ struct tba_device {
   int ordinal = 0;
   int sms = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t down = nullptr;  // device-to-host copies that overlap the next slice's upload and kernel
   std::mutex mu;
   std::string error;
   char* arena = nullptr;
@@ -1372,6 +1373,7 @@ tba_status tba_device_open(int ordinal, tba_device** out) {
                                                             std::to_string(prop.major) + std::to_string(prop.minor)};
     d->sms = prop.multiProcessorCount;
     CUDA_TRY(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&d->down, cudaStreamNonBlocking));
     CUDA_TRY(cudaMallocHost(&d->pinned, 64 * sizeof(double)));
     CUDA_TRY(tba::configure_kernels());
     CUDA_TRY(tba::adj_configure());
@@ -1389,12 +1391,14 @@ void tba_device_close(tba_device* d) {
   if (!d) return;
   cudaSetDevice(d->ordinal);
   if (d->stream) cudaStreamSynchronize(d->stream);
+  if (d->down) cudaStreamSynchronize(d->down);
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
   if (d->batch_graph) cudaGraphExecDestroy(d->batch_graph);
   if (d->batch_arena) cudaFree(d->batch_arena);
   if (d->arena) cudaFree(d->arena);
   if (d->pinned) cudaFreeHost(d->pinned);
   if (d->stream) cudaStreamDestroy(d->stream);
+  if (d->down) cudaStreamDestroy(d->down);
   delete d;
 }
 
@@ -1721,6 +1725,9 @@ tba_status tba_scene_read(tba_device* d, tba_scene* r, double* poses, double* po
   return TBA_OK;
 }
 
+// Rows per slice of an inverse-depth call (2,048 tiles of 128 rows; at most 8 slices a call).
+constexpr uint32_t kIdSliceRows = 1u << 18;
+
 tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const double* measurements,
                                        size_t measurements_len, double* linearizations, size_t linearizations_len,
                                        tba_observation_report* report) {
@@ -1753,31 +1760,54 @@ tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const doub
     double* dout = reinterpret_cast<double*>(d->arena + o_out);
     uint32_t* derr = reinterpret_cast<uint32_t*>(d->arena + o_err);
     uint32_t err = 0;
-    cudaStream_t s = d->stream;
-    cudaEvent_t e0 = event(d, 0), e1 = event(d, 1), e2 = event(d, 2), e3 = event(d, 3);
+    cudaStream_t s = d->stream, down = d->down;
+    // Slices of whole 128-row tiles (so every slice's rows start 16-byte aligned in both arrays):
+    // slice j's upload and kernel run on the main stream, its download on the second stream once
+    // its kernel is done, so downloads overlap the next slices' uploads (the link is full duplex)
+    // and the call takes about one upload plus one slice's kernel and download.
+    const uint32_t slices = count <= kIdSliceRows ? 1u : std::min<uint32_t>(8u, (count + kIdSliceRows - 1) / kIdSliceRows);
+    const uint32_t per = slices == 1 ? count : ((count + slices - 1) / slices + 127) / 128 * 128;
+    // Events: per slice [upload start, upload end = kernel start, kernel end, download start,
+    // download end], then the call's end on the second stream.
     CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(uint32_t), s));
-    CUDA_TRY(cudaEventRecord(e0, s));
-    if (count) CUDA_TRY(cudaMemcpyAsync(din, measurements, 34 * sizeof(double) * count, cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaEventRecord(e1, s));
-    CUDA_TRY(tba::launch_linearize_inverse_depth(count, din, dout, derr, d->sms, s));
-    CUDA_TRY(cudaEventRecord(e2, s));
-    if (count) CUDA_TRY(cudaMemcpyAsync(linearizations, dout, 23 * sizeof(double) * count, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaEventRecord(e3, s));
+    uint32_t launched = 0;
+    for (uint32_t j = 0, first = 0; first < count; j++, first += per) {
+      const uint32_t n = std::min(per, count - first);
+      cudaEvent_t ev[5];
+      for (int k = 0; k < 5; k++) ev[k] = event(d, 5 * size_t(j) + k);
+      CUDA_TRY(cudaEventRecord(ev[0], s));
+      CUDA_TRY(cudaMemcpyAsync(din + 34 * size_t(first), measurements + 34 * size_t(first), 34 * sizeof(double) * n,
+                               cudaMemcpyHostToDevice, s));
+      CUDA_TRY(cudaEventRecord(ev[1], s));
+      CUDA_TRY(tba::launch_linearize_inverse_depth(n, din + 34 * size_t(first), dout + 23 * size_t(first), derr,
+                                                   d->sms, s));
+      launched++;
+      CUDA_TRY(cudaEventRecord(ev[2], s));
+      CUDA_TRY(cudaStreamWaitEvent(down, ev[2], 0));
+      CUDA_TRY(cudaEventRecord(ev[3], down));
+      CUDA_TRY(cudaMemcpyAsync(linearizations + 23 * size_t(first), dout + 23 * size_t(first),
+                               23 * sizeof(double) * n, cudaMemcpyDeviceToHost, down));
+      CUDA_TRY(cudaEventRecord(ev[4], down));
+    }
     CUDA_TRY(cudaMemcpyAsync(&err, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaStreamSynchronize(down));
     if (err) throw Fail{TBA_ERROR_CUDA, "Inverse-depth linearization: a tile load did not complete"};
     if (report) {
       std::memset(report, 0, sizeof *report);
-      float ms = 0;
-      CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-      report->upload_ms = ms;
-      CUDA_TRY(cudaEventElapsedTime(&ms, e1, e2));
-      report->evaluate_ms = ms;
-      CUDA_TRY(cudaEventElapsedTime(&ms, e2, e3));
-      report->download_ms = ms;
+      // Sums over the slices (the phases of different slices overlap).
+      for (uint32_t j = 0; j < launched; j++) {
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, event(d, 5 * size_t(j)), event(d, 5 * size_t(j) + 1)));
+        report->upload_ms += ms;
+        CUDA_TRY(cudaEventElapsedTime(&ms, event(d, 5 * size_t(j) + 1), event(d, 5 * size_t(j) + 2)));
+        report->evaluate_ms += ms;
+        CUDA_TRY(cudaEventElapsedTime(&ms, event(d, 5 * size_t(j) + 3), event(d, 5 * size_t(j) + 4)));
+        report->download_ms += ms;
+      }
       report->h2d_bytes = 34ull * 8 * count;
       report->d2h_bytes = 23ull * 8 * count;
-      report->kernel_launches = count ? 1 : 0;
+      report->kernel_launches = launched;
       report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
     }
   } catch (const Fail& f) {

@@ -300,8 +300,8 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
     }
   }
   __syncthreads();
-  uint32_t k = 0;
-  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, k++) {
+  uint32_t k = 0, tile = blockIdx.x;
+  for (; tile < tiles; tile += gridDim.x, k++) {
     const uint32_t s = k % kIdStages, parity = (k / kIdStages) & 1;
     const uint32_t n = rows_of(tile);
     if (!id_wait(smem_addr(bars + s), parity)) {
@@ -331,6 +331,12 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
                      rows_of(next) * kIdIn * 8);
     }
   }
+  // After a load that did not complete in time, let this block's loads still in flight (the
+  // aborted tile's and those issued ahead of it) land before its shared memory is released; each
+  // wait is bounded.
+  if (abort_flag && producer)
+    for (uint32_t j = 0; j < uint32_t(kIdStages); j++)
+      if (tile + j * gridDim.x < tiles) id_wait(smem_addr(bars + (k + j) % kIdStages), ((k + j) / kIdStages) & 1);
   if (producer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
