@@ -287,7 +287,10 @@ def perturbed_scene(count=30, views=4, seed_noise=0.1):
 ])
 def test_package_steps_match_the_oracle_steps(options):
     inp = perturbed_scene()
-    assert_same_solve(product_ba(inp, [], options), BA(inp, [], options))
+    before = copy.deepcopy(inp)
+    got = product_ba(inp, [], options)
+    assert repr(inp) == repr(before)
+    assert_same_solve(got, BA(inp, [], options))
 
 
 def test_package_steps_match_past_convergence():

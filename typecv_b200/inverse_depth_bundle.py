@@ -30,7 +30,6 @@ here they go to the device like the linearisations.
 """
 from __future__ import annotations
 
-import copy
 import math
 from typing import Any, Generator
 
@@ -299,9 +298,10 @@ def _as_rows(answer, n: int) -> np.ndarray:
 def inverse_depth_bundle_steps(inp: dict, constraints=(), options: dict | None = None
                                ) -> Generator[dict, Any, dict[str, Any]]:
     """inverseDepthBundleSteps (inverse-depth-bundle.ts:196-565)."""
+    # The input is read, never written: results are new records (sharing the input's observation
+    # lists, as the reference's object spreads do).
     options = dict(options or {})
-    inp = copy.deepcopy(inp)
-    constraints = copy.deepcopy(list(constraints))
+    constraints = list(constraints)
     if options.get("variableViewIds") is not None:
         options["variableViewIds"] = list(options["variableViewIds"])
     if options.get("focalGroups") is not None:
@@ -458,6 +458,7 @@ def inverse_depth_bundle_steps(inp: dict, constraints=(), options: dict | None =
     accepted_steps = 0
     initial_cost = final_cost = 0.0
     last = None
+    orders: dict = {}
     for iteration in range(iterations + 1):
         blocks, n_cam = camera_blocks({"views": views}, active, scale_id if scale_free else None, origin)
         m = n_cam + len(groups)
@@ -477,7 +478,7 @@ def inverse_depth_bundle_steps(inp: dict, constraints=(), options: dict | None =
         if reduced is None:
             lam *= 10
             continue
-        factor = _factorize(reduced, linear_solver, max_factor)
+        factor = _factorize(reduced, linear_solver, max_factor, orders)
         if factor is None:
             lam *= 10
             continue
@@ -533,7 +534,7 @@ def inverse_depth_bundle_steps(inp: dict, constraints=(), options: dict | None =
     eq, m = last
     deferred = eq["deferred"]
     undamped = _reduce(eq, m, 0, dims, max_schur)
-    camera_factor = _factorize(undamped, linear_solver, max_factor) if undamped is not None else None
+    camera_factor = _factorize(undamped, linear_solver, max_factor, orders) if undamped is not None else None
     marginals = _marginals(undamped, camera_factor["inverse"], m) if camera_factor is not None else None
     estimates = []
     for index, p in enumerate(points):
@@ -723,9 +724,11 @@ def _reduce(eq: dict, m: int, lam: float, dims: np.ndarray, max_schur: int):
             "starts": eq["starts"], "m": m}
 
 
-def _factorize(reduced: dict, solver: str, max_factor: int):
+def _factorize(reduced: dict, solver: str, max_factor: int, orders: dict | None = None):
     """denseSchurFactor (inverse-depth-bundle.ts:655-668) or factorSparseSchur
-    (sparse-schur.ts:89-208): {"inverse", "entries"}, or None when a pivot fails."""
+    (sparse-schur.ts:89-208): {"inverse", "entries"}, or None when a pivot fails.  The elimination
+    order is a function of the pattern alone; ``orders`` keeps it by pattern across the LM
+    iterations of one solve, whose reduced systems mostly share their pattern."""
     m = reduced["m"]
     if solver == "dense":
         if m * m > max_factor:
@@ -737,7 +740,13 @@ def _factorize(reduced: dict, solver: str, max_factor: int):
     diagonal = np.diag(reduced["S"])
     if not np.all((diagonal > 0) & np.isfinite(diagonal)):
         return None
-    order, entries = _minimum_degree(reduced["pattern"], reduced["entries"], max_factor)
+    key = np.packbits(reduced["pattern"]).tobytes()
+    if orders is not None and key in orders:
+        order, entries = orders[key]
+    else:
+        order, entries = _minimum_degree(reduced["pattern"], reduced["entries"], max_factor)
+        if orders is not None:
+            orders[key] = (order, entries)
     inv = _factor_inverse(reduced["S"], order)
     return None if inv is None else {"inverse": inv, "entries": entries}
 
