@@ -610,13 +610,17 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 
 // STAGED: the direction of every camera (world axes, 6C values of T) is staged in shared memory
 // after the camera sums, so the per-observation read of it is an on-chip gather; one block of
-// kStagedThreads per SM.  Otherwise it is read from global memory, two blocks of kProductThreads.
+// kStagedThreads per SM.  With FP32 factors the kernel fits 64 registers and takes 1,024 threads
+// (32 warps to cover the latency of the loads each lane issues before its arithmetic): 0.157 ->
+// 0.137 ms at cfg2.  The FP64 kernel needs 80 and stays at 768 (at 1,024 it spills and the busier
+// L1 data pipe makes it slower, 0.196 -> 0.204 ms).  Otherwise it is read from global memory, two blocks of kProductThreads.
 // Both shared arrays are component-major (the sums: value j of camera c at j * C + c; the direction:
 // pair k of camera c at k * C + c, read as one 16- or 8-byte word): the lanes of a warp touch random
 // cameras, and with camera-major records of 6 words the 8-byte accesses of a warp would fall on only
 // 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over all of them.
 template <bool SHARED, typename T, bool STAGED>
-__global__ void __launch_bounds__(STAGED ? kStagedThreads : kProductThreads, STAGED ? 1 : 2) k_product_f(Params P) {
+__global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 : kStagedThreads) : kProductThreads,
+                                  STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double4 product_smem[];
   __shared__ double focal_acc;
   if (P.state[S_CG_ACTIVE] == 0) return;
@@ -1380,7 +1384,9 @@ size_t product_smem_bytes(const Params& p) {
   return product_sums_bytes(p.C, word) + (product_staged(p) ? 6 * size_t(p.C) * word : 0);
 }
 
-int product_threads(const Params& p) { return product_staged(p) ? kStagedThreads : kProductThreads; }
+int product_threads(const Params& p) {
+  return product_staged(p) ? (p.F32 ? kStagedThreadsF32 : kStagedThreads) : kProductThreads;
+}
 
 cudaError_t configure_kernels() {
   const int bytes = kStagedSmemLimit;  // the products also hold a few static bytes
