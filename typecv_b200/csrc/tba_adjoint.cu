@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(128) k_adj_prod_cameras(AdjParams A) {
 // each warp task forms y_p = V_p^-1 sum_i W_i^T p_c for its points (one observation per lane, a
 // segmented scan per point) and scatters -W_i y_p into the block's camera sums in shared memory;
 // k_adj_columns adds the blocks' partial rows in a fixed order and U_c p_c.
-constexpr int kAdjProductThreads = 256;
+constexpr int kAdjProductThreads = 352;  // 11 warps: two blocks fill 22 of the 25 warps 80 registers allow
 constexpr int kAdjTaskObs = 32;
 
 __device__ inline void adj_wt(const double* W, const double* pc, double u[3]) {
@@ -461,18 +461,18 @@ __device__ inline void adj_scatter(double* acc, uint32_t C, uint32_t c, const do
     atomicAdd(acc + size_t(a) * C + c, -(W[3 * a] * y[0] + W[3 * a + 1] * y[1] + W[3 * a + 2] * y[2]));
 }
 
-// With few cameras (PRIVATE) every warp keeps its own copy of the camera sums, so that the warps'
-// atomic adds do not contend for the same few addresses; the copies are summed at the end.
-template <bool PRIVATE>
+// With few cameras every warp keeps its own copy of the camera sums (A.prod_copies = warps), so that
+// the warps' atomic adds do not contend for the same few addresses; with more cameras fewer copies
+// fit and warps share them (warp w adds to copy w % copies).  The copies are summed at the end.
 __global__ void __launch_bounds__(kAdjProductThreads) k_adj_product(AdjParams A) {
-  extern __shared__ double adj_smem[];  // PRIVATE: one 6C copy per warp, else one; component-major
+  extern __shared__ double adj_smem[];  // prod_copies copies of 6C values, component-major
   if (A.state[A_ACTIVE] == 0) return;
   const uint32_t C = A.C;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const uint32_t copies = PRIVATE ? uint32_t(nwarps) : 1u;
+  const uint32_t copies = A.prod_copies;
   for (uint32_t j = threadIdx.x; j < copies * 6 * C; j += blockDim.x) adj_smem[j] = 0;
   __syncthreads();
-  double* adj_acc = adj_smem + (PRIVATE ? size_t(warp) * 6 * C : 0);
+  double* adj_acc = adj_smem + size_t(uint32_t(warp) % copies) * 6 * C;
   const uint32_t tb = uint32_t(uint64_t(A.ntasks) * blockIdx.x / gridDim.x);
   const uint32_t te = uint32_t(uint64_t(A.ntasks) * (blockIdx.x + 1) / gridDim.x);
   for (uint32_t t = tb + warp; t < te; t += nwarps) {
@@ -877,29 +877,32 @@ constexpr size_t kAdjSmemLimit = 227 * 1024 - 1024;
 
 uint32_t adj_one_pass_max_cameras() { return uint32_t(kAdjSmemLimit / (6 * sizeof(double))); }
 
-// Per-warp copies of the camera sums when two blocks of them fit an SM.
-bool adj_private_sums(uint32_t C) {
-  return size_t(kAdjProductThreads / 32) * 6 * sizeof(double) * C <= kAdjSmemLimit / 2;
+// As many copies of the camera sums (one per warp at most) as let two blocks share an SM; one copy
+// when not even two fit.
+uint32_t adj_product_copies(uint32_t C) {
+  const size_t one = 6 * sizeof(double) * size_t(C ? C : 1), fit = (kAdjSmemLimit / 2) / one;
+  return fit >= 2 ? uint32_t(std::min<size_t>(kAdjProductThreads / 32, fit)) : 1u;
 }
 
+size_t adj_product_smem(uint32_t C) { return size_t(adj_product_copies(C)) * 6 * sizeof(double) * C; }
+
+// Resident blocks per SM of the one-pass product (registers and shared memory), from the runtime.
 uint32_t adj_product_blocks_per_sm(uint32_t C) {
-  const size_t bytes = (adj_private_sums(C) ? size_t(kAdjProductThreads / 32) : 1) * 6 * sizeof(double) * C;
-  return uint32_t(std::max<size_t>(1, std::min<size_t>(8, (228 * 1024) / (bytes + 1024))));
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_adj_product, kAdjProductThreads, adj_product_smem(C)) !=
+          cudaSuccess ||
+      n < 1)
+    return 1;
+  return uint32_t(n);
 }
 
 cudaError_t adj_configure() {
-  cudaError_t e = cudaFuncSetAttribute(k_adj_product<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAdjSmemLimit));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_adj_product<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAdjSmemLimit));
-  return e;
+  return cudaFuncSetAttribute(k_adj_product, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAdjSmemLimit));
 }
 
 uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
   if (a.prod_blocks) {
-    const bool priv = adj_private_sums(a.C);
-    const size_t smem = (priv ? size_t(kAdjProductThreads / 32) : 1) * 6 * sizeof(double) * a.C;
-    if (priv) k_adj_product<true><<<a.prod_blocks, kAdjProductThreads, smem, s>>>(a);
-    else k_adj_product<false><<<a.prod_blocks, kAdjProductThreads, smem, s>>>(a);
+    k_adj_product<<<a.prod_blocks, kAdjProductThreads, adj_product_smem(a.C), s>>>(a);
     k_adj_columns<<<(6 * a.C + 31) / 32, 256, 0, s>>>(a);
   } else {
     k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);

@@ -83,12 +83,14 @@ struct AdjParams {
   const uint32_t* task_obs;  // ntasks + 1
   uint32_t ntasks;
   uint32_t prod_blocks;      // 0: the two-pass product
+  uint32_t prod_copies;      // copies of the camera sums in a block's shared memory (warp w adds to w % copies)
   double* part;              // prod_blocks x 6C
 };
 
 // The largest camera count of the one-pass product (its camera sums in one block's shared memory).
 uint32_t adj_one_pass_max_cameras();
-// Blocks per SM of the one-pass product for C cameras (its shared-memory camera sums).
+// Copies of the camera sums per block of the one-pass product for C cameras, and its blocks per SM.
+uint32_t adj_product_copies(uint32_t C);
 uint32_t adj_product_blocks_per_sm(uint32_t C);
 cudaError_t adj_configure();  // the one-pass product's shared-memory limit
 

@@ -1054,6 +1054,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
                       ? std::max<uint32_t>(1, std::min<uint32_t>(tba::adj_product_blocks_per_sm(C) * uint32_t(d->sms),
                                                                  (A.ntasks + 7) / 8))
                       : 0;
+  A.prod_copies = tba::adj_product_copies(C);
   Layout L;
   const size_t o_poses = L.take<double>(12 * size_t(C)), o_points = L.take<double>(3 * size_t(P)),
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
