@@ -401,11 +401,13 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const uint32_t max_task_blocks = std::max<uint32_t>(1, 4 * uint32_t(d->sms));
   const uint32_t fblocks = tba::product_finish_blocks(p);
   // The one-pass product over stored factors when its camera sums fit shared memory; the two-pass
-  // recompute form otherwise.  The mixed form stores FP32 factors.
+  // recompute form otherwise.  The mixed form stores FP32 factors for its PCG and FP64 factors for
+  // its FP64 tail and the back-substitution.
   const bool mixed = ctl->precision == TBA_PRECISION_MIXED;
   p.factored = m <= tba::product_max_unknowns();
   p.Mpad = (M + 31) / 32 * 32;
-  const size_t factor_bytes = p.factored ? size_t(tba::kFactors) * p.Mpad * (mixed ? 4 : 8) : 0;
+  const size_t factor_bytes = p.factored ? size_t(tba::kFactors) * p.Mpad * 8 : 0;
+  const size_t factor32_bytes = p.factored && mixed ? size_t(tba::kFactors) * p.Mpad * 4 : 0;
   p.F = nullptr;
   p.F32 = mixed && p.factored ? reinterpret_cast<float*>(1) : nullptr;  // set below; selects the occupancy query
   const int per_sm = p.factored ? tba::product_blocks_per_sm(p) : 1;
@@ -421,6 +423,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_rlim = L.take<double>(C), o_cmp = L.take<uint32_t>(M), o_cmx = L.take<double>(2 * size_t(M)),
                o_pblk = L.take<double>(12 * size_t(P)), o_y = L.take<double>(4 * size_t(P)),
                o_cprod = L.take<double>(8 * max_chunks), o_F = L.take<char>(factor_bytes),
+               o_F32 = L.take<char>(factor32_bytes),
                o_pw = L.take<double>(6 * size_t(C)), o_xw = L.take<double>(6 * size_t(C)),
                o_acc = L.take<double>(p.factored ? size_t(max_prod_blocks) * m : 0), o_U = L.take<double>(21 * size_t(C)),
                o_Minv = L.take<double>(36 * size_t(C)), o_rhs = L.take<double>(6 * size_t(C)),
@@ -471,8 +474,8 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.pblk = D(o_pblk);
   p.y = D(o_y);
   p.chunk_prod = D(o_cprod);
-  p.F = p.factored && !mixed ? D(o_F) : nullptr;
-  p.F32 = p.factored && mixed ? reinterpret_cast<float*>(a + o_F) : nullptr;
+  p.F = p.factored ? D(o_F) : nullptr;
+  p.F32 = p.factored && mixed ? reinterpret_cast<float*>(a + o_F32) : nullptr;
   p.pw = D(o_pw);
   p.xw = D(o_xw);
   p.acc_part = D(o_acc);
@@ -579,9 +582,9 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   launches += 4;
   CUDA_TRY(cudaGetLastError());
   bool lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
+  // The mixed form's FP64 tail: the one-pass product over the FP64 factors (the two-pass recompute
+  // product when the engine keeps no factors).
   tba::Params tail = p;
-  tail.factored = 0;
-  tail.F = nullptr;
   tail.F32 = nullptr;
   tail.tol_inner = 0;  // the tail stops at the solve's own tolerance
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
@@ -593,7 +596,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     // PCG in chunks of guarded iterations; the read after each chunk only ends the loop early.
     uint32_t done = 0, steps_before = 0;
     // `q` selects the product: the engine's own (FP32 factors in the mixed form), or the FP64
-    // two-pass product of the mixed form's tail.  Only the engine's own products are timed.
+    // product of the mixed form's tail.  Only the engine's own products are timed.
     auto run_pcg = [&](uint32_t budget, const tba::Params& q, bool timed) {
       const size_t first_pair = product_events.size();
       uint32_t chunk = 8;
@@ -625,8 +628,8 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     run_pcg(ctl->max_cg, p, true);
     // Mixed form: FP64 iterative refinement.  The true residual of the FP32-product solution
     // restarts the PCG when it is above the tolerance, and the restarted run (with an iteration
-    // budget of its own) uses the FP64 two-pass product, which resolves what FP32 factors cannot
-    // on badly conditioned systems.
+    // budget of its own) uses the FP64 product, which resolves what FP32 factors cannot on badly
+    // conditioned systems.
     if (mixed) {
       tba::launch_refine(p, s);
       launches += 4;

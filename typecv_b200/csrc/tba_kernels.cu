@@ -26,7 +26,7 @@
 //
 // No kernel stores the Schur cross blocks W_i = w J_c^T J_p (21 words per observation).  The
 // point pass stores 12 world-axis Jacobian factors per observation instead (q~ = R^T q, R^T du,
-// R^T dv, w, jf; FP64, or FP32 in the mixed form), from which every product is a few dozen FMAs;
+// R^T dv, w, jf; FP64, and an FP32 copy in the mixed form), from which every product is a few dozen FMAs;
 // the camera passes recompute the factors from the pose, the camera, the point and the pixel.
 // Every reduction runs in a fixed order (fixed grids, fixed trees, fixed chunking), except the
 // shared-memory camera sums of k_product_f, whose FP64 atomic adds commute only up to rounding.
@@ -194,10 +194,10 @@ __device__ inline void point_obs(const Params& P, uint32_t i, uint32_t pt, doubl
     f[10] = g.jf[0];
     f[11] = g.jf[1];
     const size_t stride = P.Mpad;
+    // FP64 factors always; the mixed form's PCG reads an FP32 copy.
+    for (int k = 0; k < kFactors; k++) P.F[k * stride + i] = f[k];
     if (P.F32)
       for (int k = 0; k < kFactors; k++) P.F32[k * stride + i] = float(f[k]);
-    else
-      for (int k = 0; k < kFactors; k++) P.F[k * stride + i] = f[k];
   }
   double wjp[2][3];
   for (int row = 0; row < 2; row++)
@@ -1177,8 +1177,7 @@ __global__ void __launch_bounds__(256) k_update_cameras(Params P) {
 }
 
 // W_i^T x of one observation for the candidate update: from the stored FP64 factors when the
-// engine keeps them, else recomputed in FP64 (the mixed form keeps only FP32 factors, and the
-// back-substitution stays FP64).
+// engine keeps them (both forms), else recomputed in FP64.
 __device__ inline void update_wt(const Params& P, uint32_t i, uint32_t c, uint32_t pt, double fscale, double xf,
                                  bool shared, double t[3]) {
   t[0] = t[1] = t[2] = 0;
