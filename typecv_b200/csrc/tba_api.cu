@@ -807,7 +807,7 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
                o_out = L.take<double>(output_len), o_tasks = L.take<uint32_t>(tasks.size()),
                o_desc = L.take<tba::BatchProblem>(count), o_order = L.take<uint32_t>(count),
                o_queue = L.take<uint32_t>(4);
-  std::vector<size_t> o_tp(count), o_pb(count), o_F(count);
+  std::vector<size_t> o_tp(count), o_pb(count), o_F(count), o_F64(count);
   uint64_t M_total = 0;
   for (uint32_t k = 0; k < count; k++) {
     const tba_batch_problem& q = probs[k];
@@ -815,6 +815,7 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
     o_tp[k] = L.take<double>(3 * size_t(q.points));
     o_pb[k] = L.take<double>(12 * size_t(q.points));
     o_F[k] = L.take<char>(tba::kFactors * Mpad * factor_size);
+    o_F64[k] = L.take<char>(mixed ? tba::kFactors * Mpad * sizeof(double) : 0);  // the mixed form's FP64 copy
     M_total += q.observations;
   }
   if (d->batch_capacity < L.bytes) {
@@ -872,6 +873,7 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
     b.tpoints = reinterpret_cast<double*>(a + o_tp[k]);
     b.pblk = reinterpret_cast<double*>(a + o_pb[k]);
     b.F = a + o_F[k];
+    b.F64 = mixed ? reinterpret_cast<double*>(a + o_F64[k]) : nullptr;
     b.output = dout + q.output_offset;
     b.points = b.output + 12 * size_t(C);
   }

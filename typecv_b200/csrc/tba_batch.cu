@@ -11,8 +11,8 @@
 //   b_pcg_init, b_product_f, initializeBundleCg + bundleSchurPoint/bundleSchurCamera +
 //   b_columns, b_pcg_update  advanceBundleCg (K9-K12): the whole PCG state (6C + 1 unknowns),
 //                            the camera blocks and the preconditioner live in shared memory
-//   b_refine, b_product_r    mixed form: the FP64 residual of the FP32-factor PCG solution and
-//                            the FP64 recompute product of the restarted run
+//   b_refine, b_product_r    mixed form: the FP64 residual of the FP32-factor PCG solution (FP64
+//                            recompute product); the restarted run reads an FP64 copy of the factors
 //   b_update_cameras,        updateBundleCandidate + bundleCandidateGauge +
 //   b_update_points          normalizeBundleCandidate + bundleCandidatePartials +
 //                            acceptBundleCandidate + commitBundleCandidate (K14-K19)
@@ -207,6 +207,17 @@ __device__ __forceinline__ void b_point_obs(const BatchProblem& Q, const Sh& S, 
   F[9 * stride + i] = T(g.w);
   F[10 * stride + i] = T(g.jf[0]);
   F[11 * stride + i] = T(g.jf[1]);
+  if (sizeof(T) == 4) {  // the mixed form's FP64 copy
+    double* D = Q.F64;
+    for (int c = 0; c < 3; c++) {
+      D[c * stride + i] = g.q[0] * pose[c] + g.q[1] * pose[3 + c] + g.q[2] * pose[6 + c];
+      D[(3 + c) * stride + i] = jp[0][c];
+      D[(6 + c) * stride + i] = jp[1][c];
+    }
+    D[9 * stride + i] = g.w;
+    D[10 * stride + i] = g.jf[0];
+    D[11 * stride + i] = g.jf[1];
+  }
   double wjp[2][3];
   for (int row = 0; row < 2; row++)
     for (int j = 0; j < 3; j++) wjp[row][j] = g.w * jp[row][j];
@@ -489,17 +500,16 @@ __device__ __noinline__ void b_pcg_init(const BatchProblem& Q, Sh& S) {
   __syncthreads();
 }
 
-// The one-pass product over the stored factors: -sum_i W_i y_p in world axes into acc (plus the
+// The one-pass product over the stored factors FT: -sum_i W_i y_p in world axes into acc (plus the
 // focal share), exactly the grid engine's k_product_f restricted to one problem.
 template <bool SHARED, typename T>
-__device__ __noinline__ void b_product_f(const BatchProblem& Q, Sh& S) {
+__device__ __noinline__ void b_product_f(const BatchProblem& Q, Sh& S, const T* FT, const double* vec) {
   const uint32_t m = 6 * Q.C + (SHARED ? 1 : 0);
   for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) S.acc[j] = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const T* FT = static_cast<const T*>(Q.F);
   const size_t stride = Q.Mpad;
-  const double pf = SHARED ? S.p[m - 1] : 0.0;
+  const double pf = SHARED ? vec[m - 1] : 0.0;  // the focal element of the vector (its cameras: S.pw)
   double ef = 0;
   for (uint32_t t = warp; t < Q.ntasks; t += nw) {
     const uint32_t p0 = Q.tasks[t], p1 = Q.tasks[t + 1];
@@ -750,8 +760,16 @@ template <bool SHARED>
 __device__ __noinline__ void b_refine(const BatchProblem& Q, Sh& S) {
   double* st = S.st;
   if (!(st[S_ACTIVE] != 0 && st[S_CG_FAILED] == 0 && st[S_R0] > 0)) return;
-  b_product_r<SHARED>(Q, S, S.x);
   const uint32_t C = Q.C, n = 6 * C, m = n + (SHARED ? 1 : 0);
+  // S x over the FP64 copy of the factors when it is kept (world-axis sums of -W_i y_p), else by
+  // the recompute product (camera-axis sums of +W_i y_p).
+  const bool one_pass = Q.F64 != nullptr;
+  if (one_pass) {
+    b_world(S, C, S.x, S.pw);
+    b_product_f<SHARED, double>(Q, S, Q.F64, S.x);
+  } else {
+    b_product_r<SHARED>(Q, S, S.x);
+  }
   const double xf = SHARED ? S.x[n] : 0.0;
   double hx = 0;
   for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
@@ -760,7 +778,14 @@ __device__ __noinline__ void b_refine(const BatchProblem& Q, Sh& S) {
     const double* xc = S.x + 6 * c;
     double sx = 0;
     for (int k = 0; k < 6; k++) sx += U[sym6(r, k)] * xc[k];
-    sx -= S.acc[j];
+    if (one_pass) {
+      const double* R = S.pose + 12 * c;
+      const double* a = S.acc + 6 * c;
+      const uint32_t rr = r % 3, h = r < 3 ? 0 : 3;
+      sx += R[3 * rr] * a[h] + R[3 * rr + 1] * a[h + 1] + R[3 * rr + 2] * a[h + 2];
+    } else {
+      sx -= S.acc[j];
+    }
     if (SHARED) {
       sx += S.hcf[j] * xf;
       hx += S.hcf[j] * xc[r];
@@ -777,10 +802,11 @@ __device__ __noinline__ void b_refine(const BatchProblem& Q, Sh& S) {
     v[1] += rr * zz;
   }
   bsum_all(v, S.red);
+  b_world(S, C, S.p, S.pw);  // the restarted direction in world axes, for the one-pass product
   if (threadIdx.x == 0) {
     double residual = v[0], rho = v[1];
     if (SHARED) {
-      const double sxf = st[S_FOCAL_DIAG] * xf + v[2] - S.acc[n];
+      const double sxf = st[S_FOCAL_DIAG] * xf + v[2] + (one_pass ? S.acc[n] : -S.acc[n]);
       const double rf = st[S_FOCAL_RHS] - sxf, zf = st[S_FOCAL_INV] * rf;
       S.r[n] = rf;
       S.z[n] = zf;
@@ -887,14 +913,14 @@ __device__ __noinline__ void b_update_cameras(const BatchProblem& Q, Sh& S) {
 }
 
 // W_i^T x of one observation for the back-substitution: from the FP64 factors, or recomputed in
-// FP64 when the factors are FP32.
+// FP64 when the factors are FP32 and no FP64 copy is kept.
 template <bool SHARED, typename T>
 __device__ __forceinline__ void b_update_wt(const BatchProblem& Q, const Sh& S, uint32_t i, uint32_t c, uint32_t pt,
                                             double fscale, double xf, double t[3]) {
   t[0] = t[1] = t[2] = 0;
-  if (sizeof(T) == 8) {
+  if (sizeof(T) == 8 || Q.F64) {
     Factors<double> f;
-    load_factors(static_cast<const double*>(Q.F), Q.Mpad, i, f);
+    load_factors(sizeof(T) == 8 ? static_cast<const double*>(Q.F) : static_cast<const double*>(Q.F64), Q.Mpad, i, f);
     factor_wt(f, S.xw + 6 * c, xf, Q.active[c] != 0, false, SHARED, t);
     return;
   }
@@ -1045,15 +1071,17 @@ __device__ __forceinline__ void b_solve(const BatchProblem& Q, Sh& S) {
     b_camera_pass<SHARED>(Q, S);
     b_pcg_init<SHARED>(Q, S);
     for (uint32_t k = 0; k < S.max_cg && S.st[S_CG_ACTIVE] != 0; k++) {
-      b_product_f<SHARED, T>(Q, S);
+      b_product_f<SHARED, T>(Q, S, static_cast<const T*>(Q.F), S.p);
       b_columns<SHARED>(Q, S, true);
       b_pcg_update<SHARED>(Q, S, S.tol_inner);
     }
     if (MIXED) {
+      // The true FP64 residual, then (when it is above the tolerance) the restarted PCG on the
+      // one-pass product over the FP64 copy of the factors.
       b_refine<SHARED>(Q, S);
       for (uint32_t k = 0; k < S.max_cg && S.st[S_CG_ACTIVE] != 0; k++) {
-        b_product_r<SHARED>(Q, S, S.p);
-        b_columns<SHARED>(Q, S, false);
+        b_product_f<SHARED, double>(Q, S, Q.F64, S.p);
+        b_columns<SHARED>(Q, S, true);
         b_pcg_update<SHARED>(Q, S, 0.0);
       }
     }

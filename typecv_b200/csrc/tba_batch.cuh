@@ -31,6 +31,7 @@ struct BatchProblem {
   double* tpoints;  // 3P candidate points
   double* pblk;     // 12P: V^-1 (6), b_p (3), padding
   void* F;          // 12 x Mpad Jacobian factors (float in the mixed form, else double)
+  double* F64;      // the mixed form's FP64 copy of the factors (its FP64 tail and update); else null
   double* output;   // the result record (12C + 3P + 26 [+1])
   double* points;   // output + 12C: the working copy of the points
 };
