@@ -11,7 +11,8 @@
 //                   (filterIndexedObservationDepth, stableDepth).  One thread per track: groups of
 //                   8 lanes per track measured slower (fewer independent tracks in flight per warp);
 //                   capped at 64 registers for 8 blocks of 128 per SM (a few spilled words), which
-//                   hides more of its gathers' latency: 0.925 -> 0.873 ms for the cfg2 scene
+//                   hides more of its gathers' latency: 0.925 -> 0.873 ms over 1M tracks and
+//                   6.18M observations
 //   k_obs_partials  the inlier error sum and count of each run of 64 observations, each run summed
 //                   in order (indexedObservationPartials), then k_obs_summary sums the runs in a
 //                   fixed tree (observationSummary)
