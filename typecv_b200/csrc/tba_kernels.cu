@@ -624,7 +624,8 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
                                   STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double4 product_smem[];
   __shared__ double focal_acc;
-  if (P.state[S_CG_ACTIVE] == 0) return;
+  // It runs while the PCG is active, or, with P.refine, on the mixed form's refinement of x.
+  if (P.state[S_CG_ACTIVE] == 0 && !(P.refine && P.state[S_REFINE] != 0)) return;
   const uint32_t m = P.m, C = P.C;
   // The camera sums (6C values of T: FP64 sums for FP64 factors, FP32 sums of a block's share for
   // FP32 factors), then the staged direction: three arrays of C pairs (pair k of each camera's 6).
@@ -1002,14 +1003,22 @@ __global__ void k_pcg_direction(Params P) {
 
 // ---- Mixed form: FP64 iterative refinement of the PCG solution ----------------------------------
 //
-// After the PCG ran on the FP32-factor product, k_refine_begin marks the refinement, the two-pass
-// FP64 recompute product evaluates S x (launched with p := x), and k_refine forms the true residual
+// After the PCG ran on the FP32-factor product, k_refine_begin marks the refinement, an FP64 product
+// evaluates S x (launched with p := x: one pass over the FP64 factors, or the two-pass recompute
+// product when the engine keeps no factors), and k_refine forms the true residual
 // r = b - S x, z = M^-1 r, p = z, rho and r.r.  Its last block adds the focal row and either accepts
 // x (r.r within the tolerance: the PCG stays finished) or restarts the PCG from x with this r.
 
 __global__ void k_refine_begin(Params P) {
   double* st = P.state;
   st[S_REFINE] = (st[S_ACTIVE] != 0 && st[S_CG_FAILED] == 0 && st[S_R0] > 0) ? 1 : 0;
+}
+
+// The refinement's vector x in world axes, for the one-pass product over the FP64 factors.
+__global__ void k_refine_direction(Params P) {
+  if (P.state[S_REFINE] == 0) return;
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < P.C) to_world(P.poses + 12 * size_t(c), P.x + 6 * size_t(c), P.pw + 6 * size_t(c));
 }
 
 __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
@@ -1024,8 +1033,15 @@ __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
   double v[4] = {0, 0, 0, 0};  // r.r, r.z (camera rows), H_cf . x, observation share of the focal row
   if (mine) {
     const uint32_t c = row / 6, j = row % 6;
+    // sum_i W_i y_p of the camera: the column sum of the one-pass product's partial rows (which hold
+    // its negative; a fixed camera's rows are discarded), or the two-pass product's chunk sums.
     double sum = 0;
-    for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum += P.chunk_prod[8 * size_t(ch) + j];
+    if (P.factored) {
+      if (P.active[c] != 0)
+        for (uint32_t b = 0; b < P.prod_blocks; b++) sum -= P.acc_part[size_t(b) * P.m + row];
+    } else {
+      for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum += P.chunk_prod[8 * size_t(ch) + j];
+    }
     const double* U = P.camU + 21 * size_t(c);
     const double* xc = P.x + 6 * size_t(c);
     double ux = 0;
@@ -1039,9 +1055,14 @@ __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
     P.r[row] = rr;
     rs[threadIdx.x] = rr;
   }
-  if (P.shared)
-    for (uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x; ch < P.nchunks; ch += gridDim.x * blockDim.x)
-      v[3] += P.chunk_prod[8 * size_t(ch) + 6];
+  if (P.shared) {
+    if (P.factored)
+      for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < P.prod_blocks; b += gridDim.x * blockDim.x)
+        v[3] -= P.acc_part[size_t(b) * P.m + (P.m - 1)];
+    else
+      for (uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x; ch < P.nchunks; ch += gridDim.x * blockDim.x)
+        v[3] += P.chunk_prod[8 * size_t(ch) + 6];
+  }
   __syncthreads();
   if (mine) {
     const uint32_t jr = row % 6, base = threadIdx.x - jr;
@@ -1477,7 +1498,12 @@ void launch_refine(const Params& p, cudaStream_t s) {
   Params q = p;
   q.refine = 1;
   q.p = p.x;
-  if (p.shared) {
+  if (p.factored) {
+    // S x in one pass over the FP64 factors (kept beside the FP32 ones).
+    q.F32 = nullptr;
+    k_refine_direction<<<(p.C + 255) / 256, 256, 0, s>>>(q);
+    launch_product(q, s);
+  } else if (p.shared) {
     k_schur_points<true><<<p.task_blocks, kPointThreads, 0, s>>>(q);
     k_schur_cameras<true><<<p.nchunks, kCameraThreads, 0, s>>>(q);
   } else {
