@@ -402,7 +402,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const uint32_t fblocks = tba::product_finish_blocks(p);
   // The one-pass product over stored factors when its camera sums fit shared memory; the two-pass
   // recompute form otherwise.  The mixed form stores FP32 factors for its PCG and FP64 factors for
-  // its FP64 tail and the back-substitution.
+  // its refinement residual, its FP64 tail and the back-substitution.
   const bool mixed = ctl->precision == TBA_PRECISION_MIXED;
   p.factored = m <= tba::product_max_unknowns();
   p.Mpad = (M + 31) / 32 * 32;
