@@ -379,3 +379,40 @@ def test_package_steps_match_on_the_noisy_corridor():
     got, want = product_ba(inp, [], {"iterations": 3}), BA(inp, [], {"iterations": 3})
     assert got["diagnostics"]["finalCost"] < got["diagnostics"]["initialCost"] * 0.1
     assert_same_solve(got, want)
+
+
+def test_package_steps_match_with_small_point_chunks(monkeypatch):
+    """The point elimination and the marginals in chunks of one or a few points (the chunk bound
+    lowered) give the same solve."""
+    from typecv_b200 import inverse_depth_bundle as IDB
+    inp = long_scene(16)
+    want = BA(inp, [], {"iterations": 2})
+    monkeypatch.setattr(IDB, "CHUNK_ELEMENTS", 64)
+    assert_same_solve(product_ba(inp, [], {"iterations": 2}), want)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_minimum_degree_fill_matches_the_sparse_factor(seed):
+    """The elimination order and factor entries of the pattern-only minimum degree equal the
+    oracle's numeric sparse factor on random SPD systems with random sparsity."""
+    from oracle import inverse_depth_steps as OS
+    from typecv_b200 import inverse_depth_bundle as IDB
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(5, 40))
+    pattern = np.triu(rng.random((n, n)) < rng.uniform(0.05, 0.4), 1)
+    pattern = pattern | pattern.T | np.eye(n, dtype=bool)
+    A = np.where(pattern, rng.normal(size=(n, n)), 0.0)
+    A = np.triu(A, 1) + np.triu(A, 1).T
+    A += np.diag(np.abs(A).sum(axis=1) + 1.0)
+    S = OS.SparseSymmetric(n, 10**9)
+    for i in range(n):
+        for j in range(i, n):
+            if pattern[i, j]:
+                S.add(i, j, A[i, j])
+    f = OS.factor_sparse_schur(S, 10**9)
+    order, entries = IDB._minimum_degree(pattern, S.entries, 10**9)
+    assert entries == f.entries and list(order) == list(f.order)
+    inv = IDB._factor_inverse(A, order)
+    assert np.allclose(inv, np.linalg.inv(A), rtol=1e-10, atol=1e-12)
+    for i in range(n):
+        assert abs(f.covariance(i, i) - inv[i, i]) <= 1e-10 * inv[i, i]
