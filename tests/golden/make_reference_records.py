@@ -1,6 +1,8 @@
 """Extract the reference's recorded GPU bundle-adjustment results into reference_records.json.
 
-Run in a checkout that has the reference at REFERENCE (default /root/reference).  The records are
+    python tests/golden/make_reference_records.py <path of the reference checkout>
+
+The reference checkout's path is a required argument.  The records are
 the reference's own `bundleAdjustGpu` runs (WebGPU, emulated f64) on fixtures of
 tests/typeshade/geometry-cases.mjs, from:
 
@@ -15,7 +17,9 @@ import json
 import os
 import sys
 
-REFERENCE = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_reference_records.py <path of the reference checkout>")
+REFERENCE = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_records.json")
 
 sources = [
