@@ -54,6 +54,11 @@ typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
 /* TBA_FLAG_TIME_PRODUCTS: bracket every Schur product with CUDA events and report their total
  * device time in tba_report.product_ms (a few microseconds of host work per PCG iteration). */
 #define TBA_FLAG_TIME_PRODUCTS 1u
+/* TBA_FLAG_PRODUCT_ERROR: once, on the first PCG direction of the first LM iteration, evaluate S p
+ * with the solve's own Schur product and with the FP64 two-pass product (Jacobians recomputed from
+ * the poses, points and pixels), and report their difference in tba_report.product_error_* (for
+ * the mixed form: the FP32 product's error).  Diagnostics only: two more products per call. */
+#define TBA_FLAG_PRODUCT_ERROR 2u
 
 /*
  * The control block of one solve: the reference's `control` uniform
@@ -98,6 +103,8 @@ typedef struct {
   uint32_t product_blocks; /* blocks of the one-pass product (each writes one partial row) */
   uint32_t refinements;    /* mixed form: PCG restarts from the FP64 residual */
   double check_ms;         /* host wall time of the structural checks of the arrays (before wall_ms) */
+  double product_error_max;  /* TBA_FLAG_PRODUCT_ERROR: max |S p - (S p)_64| / max |(S p)_64|, else 0 */
+  double product_error_norm; /* TBA_FLAG_PRODUCT_ERROR: ||S p - (S p)_64|| / ||(S p)_64||, else 0 */
 } tba_report;
 
 /* Lengths, in elements, of the arrays of one problem (bundleArraySizes, bundle-host.ts:134-143):
@@ -169,24 +176,33 @@ tba_status tba_scene_read(tba_device* device, tba_scene* scene, double* poses, d
  * scene, index: device pointers to the packed arrays of tba_bundle_adjust (same layouts; only the
  *   poses, points, cameras, pixels and the obsCamera/obsPoint sections are read).  Indices are not
  *   trusted: an out-of-range one is skipped and counted.
- * result: device pointer to 4 doubles: robust cost (Huber, control->huber), sum of squared
- *   errors, observations whose projection failed (behind the camera or outside the lens model),
- *   observations with an out-of-range index.  With the same inputs this equals the initial cost
- *   and squared error of tba_bundle_adjust (state words 8 and 9; word 24 is sqrt(SSE / M)).
+ * scene_len, index_len: their lengths in elements; they must equal tba_scene_size(control) and
+ *   tba_index_size(control).
+ * result: device pointer to result_len >= 4 doubles: robust cost (Huber, control->huber), sum of
+ *   squared errors, observations whose projection failed (behind the camera or outside the lens
+ *   model), observations with an out-of-range index.  With the same inputs this equals the initial
+ *   cost and squared error of tba_bundle_adjust (state words 8 and 9; word 24 is sqrt(SSE / M)).
  * stream: the cudaStream_t to run on (NULL: the default stream).  The call is asynchronous: the
  *   result is ready when the stream reaches it.
  * message: optional buffer for the error text.
  *
+ * Before any launch the call refuses (TBA_ERROR_ARGUMENT, nothing launched) lengths that differ
+ * from the control's, and any of scene, index or result that is not device (or managed) memory of
+ * the current device or whose allocation holds fewer bytes from the pointer than its length claims
+ * (cudaPointerGetAttributes and the driver's cuMemGetAddressRange; neither allocates).
+ *
  * Limit: at most 16,777,216 observations (4,096 tiles of 4,096); larger scenes are refused with
  * TBA_ERROR_ARGUMENT.  The tile partials live in one fixed 128 KiB array that every GPU loading
- * the library holds until exit.  The first call on a device looks up that array's device address
+ * the library holds until exit.  The first call on a device (and the first after the caller's
+ * current context changes, e.g. after cudaDeviceReset) looks up that array's device address
  * (cudaGetSymbolAddress) with the caller's current device; make that first call before any stream
  * capture.  Every call shares the array: each call writes every tile row it reads, so nothing has
  * to start at zero, but calls that overlap on the GPU (different streams, not ordered) race and
  * must be serialised by the caller.
  */
-tba_status tba_scene_cost_noalloc(const tba_control* control, const double* scene, const uint32_t* index,
-                                  double* result, void* stream, char* message, size_t message_len);
+tba_status tba_scene_cost_noalloc(const tba_control* control, const double* scene, size_t scene_len,
+                                  const uint32_t* index, size_t index_len, double* result, size_t result_len,
+                                  void* stream, char* message, size_t message_len);
 
 /*
  * Batched local-window bundle adjustment: many independent problems in one persistent launch
@@ -242,6 +258,8 @@ typedef struct {
   uint32_t blocks;        /* persistent blocks launched */
   uint32_t graph_replayed; /* 1: the launch replayed a cached CUDA graph */
   uint32_t kernel_launches;
+  uint32_t form;           /* the tba_precision that ran: a mixed request runs the FP64 form when the
+                              autotuner (schedule 0) timed it faster for this batch shape */
 } tba_batch_report;
 
 /* The largest camera count of one batched problem, and the number of launch shapes. */
@@ -286,7 +304,7 @@ typedef struct {
   uint32_t anchor, scale_view;
   uint32_t newton_steps;  /* Newton iterations, 0..50 */
   uint32_t max_cg;        /* PCG iterations per linear solve, 1..100000 */
-  uint32_t flags;         /* 0 */
+  uint32_t flags;         /* 0 or TBA_VJP_FLAG_TIME_PRODUCTS */
   double huber;           /* as tba_control.huber */
   double cg_tolerance;    /* relative PCG residual of every linear solve, 1e-15..1e-2 */
 } tba_vjp_control;
@@ -308,7 +326,16 @@ typedef struct {
                                    diagonal that makes them definite (their derivatives are then
                                    approximate: such points have a nearly flat robust cost) */
   uint32_t kernel_launches;     /* kernels launched by the call */
+  double product_ms;            /* TBA_VJP_FLAG_TIME_PRODUCTS: device time of the one-pass Schur
+                                   products that ran PCG steps (CUDA events), else 0 */
+  uint32_t product_launches;    /* the products timed in product_ms */
+  uint32_t product_blocks;      /* blocks of the one-pass product (each writes one partial row); 0:
+                                   the two-pass product (camera systems beyond shared memory) */
 } tba_vjp_report;
+
+/* TBA_VJP_FLAG_TIME_PRODUCTS: bracket every one-pass Schur product of the vjp's linear solves with
+ * CUDA events and report their total in tba_vjp_report.product_ms. */
+#define TBA_VJP_FLAG_TIME_PRODUCTS 1u
 
 tba_status tba_bundle_vjp(tba_device* device, const tba_vjp_control* control, const double* scene, size_t scene_len,
                           const uint32_t* index, size_t index_len, const double* cotangent, size_t cotangent_len,
@@ -361,11 +388,27 @@ tba_status tba_evaluate_observations(tba_device* device, const tba_observation_c
  * point; the reference pose; the observing pose; the observing camera record; its squared radial
  * limit), linearizations: 23 doubles per observation (valid flag, pixel, 2x3 point derivatives,
  * 2x6 pose derivatives, 2 log-focal derivatives), the layouts the reference's host reads.  The
- * report is the observation report's shape (evaluate_ms = the kernel).
+ * report is the observation report's shape (evaluate_ms = the kernel).  A call of more than 262,144
+ * rows runs in slices whose downloads overlap the next slices' uploads only when both host arrays
+ * are page-locked (cudaHostAlloc / cudaHostRegister); with pageable arrays the copies of each slice
+ * complete before the next is issued and the slices run one after another.
+ *
+ * The kernel streams tiles through shared memory with bulk copies and waits on them with bounded
+ * polls: a wait that runs out ends the call with TBA_ERROR_CUDA ("a tile load did not complete")
+ * after the block's loads still in flight have landed, and the handle stays usable.
  */
 tba_status tba_linearize_inverse_depth(tba_device* device, uint32_t count, const double* measurements,
                                        size_t measurements_len, double* linearizations, size_t linearizations_len,
                                        tba_observation_report* report);
+
+/*
+ * Polls of each main-loop tile wait of tba_linearize_inverse_depth on this handle (default
+ * TBA_WAIT_LIMIT_DEFAULT).  No counterpart in the reference: it lets a test make the waits run out
+ * (0 polls gives up at once) to exercise the failure path; the drain of the loads in flight after
+ * such a failure always keeps the full bound.
+ */
+#define TBA_WAIT_LIMIT_DEFAULT 4194304u
+tba_status tba_device_set_wait_limit(tba_device* device, uint32_t polls);
 
 #ifdef __cplusplus
 }

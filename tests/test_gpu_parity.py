@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import typecv_b200 as tb
+from typecv_b200 import _lib
 from typecv_b200 import synthetic as S
 from oracle import bundle_adjust as ob
 from reference_cases import bundle_fixture, bundle_metrics, joint_focal_fixture, skew_bundle_fixture
@@ -181,6 +182,29 @@ def test_synthetic_ring_matches_cpu_reference(device, shared):
     assert gd["finalCost"] < gd["initialCost"] and gd["acceptedSteps"] > 0
 
 
+def test_helix_full_size_matches_cpu_reference(device):
+    # Configuration 1 at its full size: 200 cameras on a 3-lap helix, 100k points each in 3-12
+    # cameras (751,555 observations), shared focal, 30 LM iterations, PCG tolerance 1e-12 with a
+    # budget of 256 — against the exact dense CPU bundle adjustment (bundle-adjustment.ts:80-291,
+    # joint-focal.ts:45-287; a 1,201-unknown reduced system per iteration).
+    scene = S.helix_scene()
+    assert (scene.C, scene.P) == (200, 100_000) and scene.M > 700_000
+    rec = scene.as_reconstruction()
+    opts = {"iterations": 30, "huberPx": 2.0, "refineSharedFocal": True, "cgRelativeTolerance": 1e-12,
+            "maxCgIterations": 256}
+    got = tb.bundle_adjust_gpu(device, rec, opts)
+    want = ob.cpu_bundle_adjust(rec, opts)
+    gd, wd = got["diagnostics"], want["diagnostics"]
+    assert abs(gd["initialCost"] - wd["initialCost"]) <= 1e-12 * wd["initialCost"]
+    assert abs(gd["finalCost"] - wd["finalCost"]) <= COST_REL * wd["finalCost"], (gd, wd)
+    assert abs(gd["finalRmsePx"] - wd["finalRmsePx"]) <= RMS_PX, (gd, wd)
+    assert gd["acceptedSteps"] == wd["acceptedSteps"] and gd["rejectedSteps"] == wd["rejectedSteps"]
+    assert got["linearSolverFailures"] == 0
+    fx = [v["camera"]["fx"] for v in got["reconstruction"]["views"]]
+    fx_ref = [v["camera"]["fx"] for v in want["reconstruction"]["views"]]
+    assert np.max(np.abs(np.asarray(fx) / np.asarray(fx_ref) - 1)) < 1e-9
+
+
 def test_long_tracks_and_skewed_cameras(device):
     # Points seen by more than 32 cameras take the multi-round warp path.
     scene = S.ring_scene(seed=3, cameras=40, points=200)
@@ -243,6 +267,31 @@ def test_mixed_precision_reaches_the_fp64_cost(device, kind):
         assert abs(c32 - cr) <= MIXED_REL * cr, (c32, cr)
         assert o32[base + 10] > 0 and o32[base + 17] == 0
         assert np.max(np.abs(o32[:12 * scene.C] - o64[:12 * scene.C])) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["ring", "helix"])
+def test_schur_product_error_against_the_fp64_two_pass_product(device, kind):
+    # On the first PCG direction of the first LM iteration, S p from the solve's own product against
+    # the FP64 two-pass product (Jacobians recomputed from poses, points and pixels): the FP64
+    # one-pass product over stored factors differs by rounding only; the mixed form's FP32 product
+    # (FP32 factors, FP32 warp segment sums, FP64 sums across segments) by its FP32 error, which the
+    # FP64 refinement of each PCG solution then removes.
+    scene = S.ring_scene(seed=11) if kind == "ring" else S.helix_scene(cameras=40, points=4000)
+    s, i = scene.packed()
+    errors = {}
+    for precision in (0, 1):
+        for shared in (True, False):
+            ctl = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, iterations=2,
+                                  shared_focal=shared, tolerance=1e-8, max_cg=200, precision=precision,
+                                  flags=_lib.TBA_FLAG_PRODUCT_ERROR)
+            _, rep = tb.solve_packed(device, ctl, s, i)
+            errors[(precision, shared)] = (rep["product_error_max"], rep["product_error_norm"])
+    print(f"{kind}: product error (max, norm) {errors}")
+    for shared in (True, False):
+        fp64_max, fp64_norm = errors[(0, shared)]
+        mixed_max, mixed_norm = errors[(1, shared)]
+        assert fp64_max < 1e-12 and fp64_norm < 1e-12, errors
+        assert 0 < mixed_norm < 1e-5 and mixed_max < 1e-4, errors
 
 
 def test_mixed_precision_through_the_operator(device):

@@ -162,3 +162,35 @@ def test_sliced_call_matches_the_oracle(device):
     assert np.max(np.abs(out["out"][ok] - want[ok]) / np.maximum(1, np.abs(want[ok]))) < 1e-8
     again = ID.linearize_rows(device, rows, 262_145)
     assert again["batches"] == 3 and np.array_equal(again["out"], out["out"])
+
+
+def test_tile_wait_that_runs_out_reports_an_error_and_the_handle_recovers(device):
+    # The kernel's bounded mbarrier waits are its failure detection.  With the main-loop waits cut
+    # to zero polls, every block gives up on its first tile at once; the loads it issued still land
+    # (the drain keeps the full bound), the call returns TBA_ERROR_CUDA with its message, and the
+    # next call on the same handle, at the default bound, is correct.
+    import ctypes
+
+    from typecv_b200 import _lib
+    from typecv_b200.synthetic import inverse_depth_rows
+    lib = _lib.load()
+    n = 3000  # 24 tiles: several blocks, each with both stages loaded when its first wait fails
+    rows = np.ascontiguousarray(inverse_depth_rows(measurements=n).ravel())
+    out = np.full(23 * n, np.nan)
+
+    def call():
+        return lib.tba_linearize_inverse_depth(device.handle, n, _lib.dptr(rows), rows.size, _lib.dptr(out), out.size,
+                                               ctypes.byref(_lib.ObservationReport()))
+
+    try:
+        assert lib.tba_device_set_wait_limit(device.handle, 0) == _lib.TBA_OK
+        assert call() == _lib.TBA_ERROR_CUDA
+        msg = lib.tba_last_error(device.handle).decode()
+        assert "did not complete" in msg and "in flight" not in msg, msg
+    finally:
+        assert lib.tba_device_set_wait_limit(device.handle, _lib.TBA_WAIT_LIMIT_DEFAULT) == _lib.TBA_OK
+    out[:] = np.nan
+    assert call() == _lib.TBA_OK, lib.tba_last_error(device.handle)
+    want = oid.linearize_rows(rows.reshape(n, 34))
+    got = out.reshape(n, 23)
+    assert np.max(np.abs(got - want) / np.maximum(1, np.abs(want))) < 1e-8

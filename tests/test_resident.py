@@ -1,12 +1,17 @@
 """The resident scene (tba_scene_*): an adjustment on device-resident arrays gives the result of
-tba_bundle_adjust on the same arrays, leaves its solution in the scene for the next adjustment,
-and uploads nothing of the problem per call."""
+tba_bundle_adjust on the same arrays and of the reference operator's algorithm restated on the CPU
+(the oracle, as packBundleScene feeds it: src/sfm/bundle/gpu/bundle-host.ts:177-218), leaves its
+solution in the scene for the next adjustment, and uploads nothing of the problem per call."""
 import numpy as np
 import pytest
 
 import typecv_b200 as tb
+from oracle import bundle_adjust as ob
 from typecv_b200 import synthetic as S
 from typecv_b200.resident import ResidentScene
+
+COST_REL = 1e-9  # final robust cost, FP64 form
+POSE_TOL = 1e-7
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +42,33 @@ def test_resident_adjustments_chain_like_separate_calls(device):
         want2, _ = tb.solve_packed(device, ctl, s2, i)
         assert abs(st2[6] - want2[n + 6]) <= 1e-9 * want2[n + 6]
         assert st2[6] <= st1[6]
+
+
+@pytest.mark.parametrize("shared", [False, True])
+def test_resident_chain_matches_the_operator_oracle(device, shared):
+    # Two chained adjustments of one resident scene against the oracle run twice, the second time
+    # on the oracle's own first solution: same accepted steps, costs within 1e-9, poses within 1e-7.
+    # A resident scene carries poses and points from one adjustment to the next; its camera records
+    # (and so the focal scale's starting point) stay as created, as they do here for the oracle.
+    sc = S.helix_scene(seed=43, cameras=24, points=2500)
+    s, i = sc.packed()
+    C, P = sc.C, sc.P
+    n = 12 * C + 3 * P
+    ctl = tb.make_control(C, P, sc.M, anchor=0, scale_view=1, iterations=5, shared_focal=shared)
+    kw = dict(iterations=5, huber=2.0, max_cg=ctl.max_cg, shared=shared)
+    ref1 = ob.gpu_operator_packed({"C": C, "P": P, "M": sc.M, "scene": s, "index": i}, 0, 1, **kw)
+    s_ref = s.copy()
+    s_ref[:n] = ref1[:n]
+    ref2 = ob.gpu_operator_packed({"C": C, "P": P, "M": sc.M, "scene": s_ref, "index": i}, 0, 1, **kw)
+    with ResidentScene(device, ctl, s, i) as rs:
+        out1, _, _ = rs.adjust(output=True)
+        _, st2, _ = rs.adjust()
+        poses2, points2 = rs.read()
+    for got, want in ((out1[n:n + 26], ref1[n:n + 26]), (st2[:26], ref2[n:n + 26])):
+        assert abs(got[6] - want[6]) <= COST_REL * want[6], (got[6], want[6])
+        assert got[10] == want[10] and got[11] == want[11]  # accepted, rejected
+    assert np.max(np.abs(out1[:12 * C] - ref1[:12 * C])) < POSE_TOL
+    assert np.max(np.abs(poses2 - ref2[:12 * C])) < POSE_TOL
 
 
 def test_resident_write_read_and_shape_checks(device):

@@ -21,10 +21,13 @@ COST_REL = 1e-9  # the FP64 cost tolerance of the parity tests
 RMS_PX = 1e-6
 
 
-def _noalloc(lib, control, scene_dev, index_dev, result_dev):
+def _noalloc(lib, control, scene_ptr, index_ptr, result_ptr, scene_len=None, index_len=None, result_len=4):
+    """One call through the C ABI; pointers are device addresses (ints), lengths default to the control's."""
     msg = ctypes.create_string_buffer(512)
-    status = lib.tba_scene_cost_noalloc(ctypes.byref(control), scene_dev.data_ptr(), index_dev.data_ptr(),
-                                        result_dev.data_ptr(), None, msg, len(msg))
+    scene_len = lib.tba_scene_size(ctypes.byref(control)) if scene_len is None else scene_len
+    index_len = lib.tba_index_size(ctypes.byref(control)) if index_len is None else index_len
+    status = lib.tba_scene_cost_noalloc(ctypes.byref(control), scene_ptr, scene_len, index_ptr, index_len,
+                                        result_ptr, result_len, None, msg, len(msg))
     return status, msg.value.decode()
 
 
@@ -44,7 +47,7 @@ def test_noalloc_cost_matches_the_allocating_entry_point_on_two_calls():
             scene_dev = torch.from_numpy(s).cuda()
             index_dev = torch.from_numpy(i.view(np.int32)).cuda()
             result_dev = torch.full((4,), -1.0, dtype=torch.float64, device="cuda")
-            status, msg = _noalloc(lib, control, scene_dev, index_dev, result_dev)
+            status, msg = _noalloc(lib, control, scene_dev.data_ptr(), index_dev.data_ptr(), result_dev.data_ptr())
             assert status == _lib.TBA_OK, msg
             torch.cuda.synchronize()
             cost, squares, failed, bad = result_dev.cpu().numpy()
@@ -58,5 +61,44 @@ def test_noalloc_refuses_scenes_beyond_its_scratch():
     lib = _lib.load()
     big = tb.make_control(2, 1, 16_777_217, anchor=0, scale_view=1, huber=2.0)
     dummy = torch.zeros(8, dtype=torch.float64, device="cuda")
-    status, msg = _noalloc(lib, big, dummy, dummy, dummy)
+    status, msg = _noalloc(lib, big, dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr())
     assert status == _lib.TBA_ERROR_ARGUMENT and "16777216" in msg
+
+
+def test_noalloc_refuses_host_memory_and_short_buffers_before_any_launch():
+    # Each refused call returns before launching anything, so the result buffer keeps its marker
+    # and the context stays usable for the valid call at the end.
+    import torch
+    lib = _lib.load()
+    scene = S.ring_scene(cameras=6, points=300)
+    s, i = scene.packed()
+    control = tb.make_control(scene.C, scene.P, scene.M, anchor=0, scale_view=1, huber=2.0)
+    scene_dev = torch.from_numpy(s).cuda()
+    index_dev = torch.from_numpy(i.view(np.int32)).cuda()
+    result_dev = torch.full((4,), -1.0, dtype=torch.float64, device="cuda")
+    host_result = np.full(4, -1.0)
+    cases = [
+        # host memory in place of each device buffer
+        ((s.ctypes.data, index_dev.data_ptr(), result_dev.data_ptr()), {}, "scene is host memory"),
+        ((scene_dev.data_ptr(), i.ctypes.data, result_dev.data_ptr()), {}, "index is host memory"),
+        ((scene_dev.data_ptr(), index_dev.data_ptr(), host_result.ctypes.data), {}, "result is host memory"),
+        # lengths that differ from the control's
+        ((scene_dev.data_ptr(), index_dev.data_ptr(), result_dev.data_ptr()), {"scene_len": s.size - 1}, "lengths"),
+        ((scene_dev.data_ptr(), index_dev.data_ptr(), result_dev.data_ptr()), {"index_len": i.size + 1}, "lengths"),
+        ((scene_dev.data_ptr(), index_dev.data_ptr(), result_dev.data_ptr()), {"result_len": 3}, "lengths"),
+    ]
+    for ptrs, lens, text in cases:
+        status, msg = _noalloc(lib, control, *ptrs, **lens)
+        assert status == _lib.TBA_ERROR_ARGUMENT and text in msg, (text, msg)
+    # A control claiming far more observations than the caller's device buffers hold: the lengths
+    # agree with the control, the allocations do not.
+    big = tb.make_control(scene.C, scene.P, 8_000_000, anchor=0, scale_view=1, huber=2.0)
+    small = torch.zeros(1024, dtype=torch.float64, device="cuda")
+    status, msg = _noalloc(lib, big, small.data_ptr(), small.data_ptr(), result_dev.data_ptr())
+    assert status == _lib.TBA_ERROR_ARGUMENT and "allocation holds" in msg, msg
+    torch.cuda.synchronize()
+    assert np.all(result_dev.cpu().numpy() == -1.0) and np.all(host_result == -1.0)
+    status, msg = _noalloc(lib, control, scene_dev.data_ptr(), index_dev.data_ptr(), result_dev.data_ptr())
+    assert status == _lib.TBA_OK, msg
+    torch.cuda.synchronize()
+    assert result_dev.cpu().numpy()[0] > 0

@@ -14,13 +14,16 @@ LIB_PATH = os.path.join(HERE, "libtba.so")
 TBA_OK, TBA_ERROR_ARGUMENT, TBA_ERROR_BUDGET, TBA_ERROR_CUDA, TBA_ERROR_INTERNAL = range(5)
 TBA_PRECISION_FP64, TBA_PRECISION_MIXED = 0, 1
 TBA_FLAG_TIME_PRODUCTS = 1
+TBA_FLAG_PRODUCT_ERROR = 2
+TBA_VJP_FLAG_TIME_PRODUCTS = 1
+TBA_WAIT_LIMIT_DEFAULT = 4194304
 
 # Every symbol include/tba.h declares.
 EXPORTS = ("tba_scene_size", "tba_index_size", "tba_output_size", "tba_device_open", "tba_device_close",
            "tba_last_error", "tba_bundle_adjust", "tba_scene_cost_noalloc", "tba_batch_max_cameras",
            "tba_batch_shapes", "tba_batch_shape", "tba_batch_adjust", "tba_bundle_vjp",
            "tba_evaluate_observations", "tba_scene_create", "tba_scene_destroy", "tba_scene_adjust",
-           "tba_scene_write", "tba_scene_read", "tba_linearize_inverse_depth")
+           "tba_scene_write", "tba_scene_read", "tba_linearize_inverse_depth", "tba_device_set_wait_limit")
 
 
 class LibraryError(RuntimeError):
@@ -46,6 +49,7 @@ class Report(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint32), ("lm_iterations", ctypes.c_uint32),
         ("cg_iterations", ctypes.c_uint32), ("product_launches", ctypes.c_uint32), ("engine", ctypes.c_uint32),
         ("product_blocks", ctypes.c_uint32), ("refinements", ctypes.c_uint32), ("check_ms", ctypes.c_double),
+        ("product_error_max", ctypes.c_double), ("product_error_norm", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -76,6 +80,7 @@ class BatchReport(ctypes.Structure):
         ("lm_iterations", ctypes.c_uint64), ("cg_iterations", ctypes.c_uint64),
         ("problems", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("threads", ctypes.c_uint32),
         ("blocks", ctypes.c_uint32), ("graph_replayed", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+        ("form", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -98,6 +103,7 @@ class VjpReport(ctypes.Structure):
         ("adjoint_residual", ctypes.c_double),
         ("cg_iterations", ctypes.c_uint32), ("newton_steps", ctypes.c_uint32), ("failed", ctypes.c_uint32),
         ("invalid", ctypes.c_uint32), ("point_failures", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+        ("product_ms", ctypes.c_double), ("product_launches", ctypes.c_uint32), ("product_blocks", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -154,7 +160,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tba_bundle_adjust.argtypes = [vp, P(Control), P(ctypes.c_double), ctypes.c_size_t, P(ctypes.c_uint32),
                                       ctypes.c_size_t, P(ctypes.c_double), ctypes.c_size_t, P(Report)]
     lib.tba_scene_cost_noalloc.restype = ctypes.c_int
-    lib.tba_scene_cost_noalloc.argtypes = [P(Control), vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t]
+    lib.tba_scene_cost_noalloc.argtypes = [P(Control), vp, ctypes.c_size_t, vp, ctypes.c_size_t, vp, ctypes.c_size_t,
+                                           vp, ctypes.c_char_p, ctypes.c_size_t]
     lib.tba_batch_max_cameras.restype = ctypes.c_uint32
     lib.tba_batch_max_cameras.argtypes = []
     lib.tba_batch_shapes.restype = ctypes.c_uint32
@@ -191,6 +198,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tba_linearize_inverse_depth.restype = ctypes.c_int
     lib.tba_linearize_inverse_depth.argtypes = [vp, ctypes.c_uint32, P(ctypes.c_double), ctypes.c_size_t,
                                                 P(ctypes.c_double), ctypes.c_size_t, P(ObservationReport)]
+    lib.tba_device_set_wait_limit.restype = ctypes.c_int
+    lib.tba_device_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
     _lib = lib
     return lib
 

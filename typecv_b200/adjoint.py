@@ -19,13 +19,16 @@ from .bundle import DeviceError, RangeError, ShadeDevice
 
 def bundle_vjp(device: ShadeDevice, C: int, P: int, M: int, scene: np.ndarray, index: np.ndarray,
                cotangent: np.ndarray | None, *, anchor: int = 0, scale_view: int = 1, newton_steps: int = 0,
-               max_cg: int = 5000, tolerance: float = 1e-12, huber: float = 2.0, want_solution: bool = False):
+               max_cg: int = 5000, tolerance: float = 1e-12, huber: float = 2.0, want_solution: bool = False,
+               time_products: bool = False):
     """Returns (pixels_bar (M x 2) or None, intrinsics_bar (d/ds, d/dk1) or None, solution or None,
-    report dict).  `scene` holds the evaluation point (poses and points) and the observations."""
+    report dict).  `scene` holds the evaluation point (poses and points) and the observations.
+    `time_products` brackets each one-pass Schur product with CUDA events (report product_ms)."""
     lib = _lib.load()
     scene = np.ascontiguousarray(scene, dtype=np.float64)
     index = np.ascontiguousarray(index, dtype=np.uint32)
-    ctl = _lib.VjpControl(C, P, M, anchor, scale_view, newton_steps, max_cg, 0, huber, tolerance)
+    flags = _lib.TBA_VJP_FLAG_TIME_PRODUCTS if time_products else 0
+    ctl = _lib.VjpControl(C, P, M, anchor, scale_view, newton_steps, max_cg, flags, huber, tolerance)
     n_theta = 12 * C + 3 * P
     report = _lib.VjpReport()
     ybar = np.zeros(2 * M) if cotangent is not None else None

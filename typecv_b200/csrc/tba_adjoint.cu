@@ -900,9 +900,11 @@ cudaError_t adj_configure() {
   return cudaFuncSetAttribute(k_adj_product, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAdjSmemLimit));
 }
 
-uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s) {
+uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s, cudaEvent_t before, cudaEvent_t after) {
   if (a.prod_blocks) {
+    if (before) cudaEventRecord(before, s);
     k_adj_product<<<a.prod_blocks, kAdjProductThreads, adj_product_smem(a.C), s>>>(a);
+    if (after) cudaEventRecord(after, s);
     k_adj_columns<<<(6 * a.C + 31) / 32, 256, 0, s>>>(a);
   } else {
     k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);

@@ -98,7 +98,9 @@ uint32_t adj_launch_init(const AdjParams& a, cudaStream_t s);        // gauge or
 uint32_t adj_launch_reset(const AdjParams& a, cudaStream_t s);       // zero the per-solve sums and flags
 uint32_t adj_launch_assemble(const AdjParams& a, cudaStream_t s);    // per observation, points, cameras
 uint32_t adj_launch_pcg_init(const AdjParams& a, cudaStream_t s);
-uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s);    // product + vector step
+// Product + vector step; with events, the one-pass product's launch is bracketed by them.
+uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s, cudaEvent_t before = nullptr,
+                             cudaEvent_t after = nullptr);
 uint32_t adj_launch_back_substitute(const AdjParams& a, cudaStream_t s);
 // The candidate theta (+) delta into tposes/tpoints (with the gauge normalisation) and its robust
 // cost into A_COST; then, when accepted, its commit.

@@ -40,6 +40,8 @@ struct tba_device {
   size_t capacity = 0;
   double* pinned = nullptr;  // small host buffer for flag reads
   std::vector<cudaEvent_t> events;
+  // Polls of each main-loop wait of the inverse-depth linearisation (tba_device_set_wait_limit).
+  uint32_t wait_limit = tba::kIdWaitPolls;
   // Batched solves: their own workspace, the cached graph of the last launch and its key, and
   // the autotuner's choices by batch shape.
   char* batch_arena = nullptr;
@@ -332,9 +334,66 @@ cudaEvent_t event(tba_device* d, size_t k) {
   return d->events[k];
 }
 
-// The host-side schedules of one problem's index: warp tasks (with their first observations),
+// Stable counting sort of the point ids `in` by key[id] (< buckets) into `out`, on host threads:
+// per-thread histograms of contiguous ranges, offsets bucket-major then thread, ranges scattered in
+// order.
+void bucket_pass(const uint32_t* in, uint32_t n, const uint32_t* key, uint32_t buckets, uint32_t* out) {
+  const unsigned threads = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<uint32_t> hist(size_t(threads) * buckets, 0);
+  const uint64_t serial_below = 1u << 16;
+  parallel_ranges(n, serial_below, [&](uint64_t b, uint64_t e, unsigned t) {
+    uint32_t* h = hist.data() + size_t(t) * buckets;
+    for (uint64_t i = b; i < e; i++) h[key[in[i]]]++;
+  });
+  uint32_t run = 0;
+  for (uint32_t b = 0; b < buckets; b++)
+    for (unsigned t = 0; t < threads; t++) {
+      const uint32_t count = hist[size_t(t) * buckets + b];
+      hist[size_t(t) * buckets + b] = run;
+      run += count;
+    }
+  parallel_ranges(n, serial_below, [&](uint64_t b, uint64_t e, unsigned t) {
+    uint32_t* h = hist.data() + size_t(t) * buckets;
+    for (uint64_t i = b; i < e; i++) out[h[key[in[i]]]++] = in[i];
+  });
+}
+
+// The engine's point order (tba_engine.cuh): the finite points sorted by the smallest, then the
+// largest camera observing them, stably; the directional points last, in their order.  Empty
+// (the caller's order) when the point offsets are not well formed; the device checks then fail the
+// problem before any kernel reads a schedule.
+std::vector<uint32_t> order_points(const uint32_t* obs_camera, const uint32_t* ps, uint32_t C, uint32_t P, uint32_t D,
+                                   uint32_t M) {
+  if (P == 0 || D > P || ps[0] != 0 || ps[P] != M) return {};
+  for (uint32_t p = 0; p < P; p++)
+    if (ps[p] > ps[p + 1]) return {};
+  const uint32_t F = P - D;
+  std::vector<uint32_t> lo(F), hi(F);
+  parallel_ranges(F, 1u << 15, [&](uint64_t b, uint64_t e, unsigned) {
+    for (uint64_t p = b; p < e; p++) {
+      uint32_t a = C - 1, z = 0;
+      for (uint32_t k = ps[p]; k < ps[p + 1]; k++) {
+        const uint32_t c = std::min(obs_camera[k], C - 1);  // out-of-range ids fail the checks later
+        a = std::min(a, c);
+        z = std::max(z, c);
+      }
+      lo[p] = a;
+      hi[p] = z;
+    }
+  });
+  std::vector<uint32_t> ids(F), by_hi(F), order(P);
+  std::iota(ids.begin(), ids.end(), 0u);
+  bucket_pass(ids.data(), F, hi.data(), C, by_hi.data());
+  bucket_pass(by_hi.data(), F, lo.data(), C, order.data());
+  for (uint32_t p = F; p < P; p++) order[p] = p;
+  return order;
+}
+
+// The host-side schedules of one problem's index: the engine's point order with the first
+// observation of each position, warp tasks over that order (with their first observations),
 // camera chunks and the number of fixed cameras.
 struct HostPlan {
+  std::vector<uint32_t> order, pstart;  // empty order: the caller's order (pstart then unused)
   std::vector<uint32_t> tasks, task_obs;
   Chunks chunks;
   uint32_t fixed = 0;
@@ -346,9 +405,17 @@ HostPlan make_plan(const tba_control* ctl, const uint32_t* index, int sms) {
   const uint32_t* cs = ps + P + 1;
   const uint32_t* active = cs + C + 1 + M;
   HostPlan plan;
-  plan.tasks = build_tasks(ps, P);
+  plan.order = order_points(index, ps, C, P, ctl->directional_points, M);
+  const uint32_t* starts = ps;
+  if (!plan.order.empty()) {
+    plan.pstart.resize(size_t(P) + 1);
+    plan.pstart[0] = 0;
+    for (uint32_t q = 0; q < P; q++) plan.pstart[q + 1] = plan.pstart[q] + (ps[plan.order[q] + 1] - ps[plan.order[q]]);
+    starts = plan.pstart.data();
+  }
+  plan.tasks = build_tasks(starts, P);
   plan.task_obs.resize(plan.tasks.size());
-  for (size_t t = 0; t < plan.tasks.size(); t++) plan.task_obs[t] = ps[plan.tasks[t]];
+  for (size_t t = 0; t < plan.tasks.size(); t++) plan.task_obs[t] = starts[plan.tasks[t]];
   plan.chunks = build_chunks(cs, C, M, sms);
   for (uint32_t c = 0; c < C; c++) plan.fixed += active[c] == 0;
   return plan;
@@ -406,7 +473,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const bool mixed = ctl->precision == TBA_PRECISION_MIXED;
   p.factored = m <= tba::product_max_unknowns();
   p.Mpad = (M + 31) / 32 * 32;
-  const size_t factor_bytes = p.factored ? size_t(tba::kFactors) * p.Mpad * 8 : 0;
+  const size_t factor_bytes = p.factored && !mixed ? size_t(tba::kFactors) * p.Mpad * 8 : 0;
   const size_t factor32_bytes = p.factored && mixed ? size_t(tba::kFactors) * p.Mpad * 4 : 0;
   p.F = nullptr;
   p.F32 = mixed && p.factored ? reinterpret_cast<float*>(1) : nullptr;  // set below; selects the occupancy query
@@ -417,6 +484,9 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
                o_tposes = L.take<double>(12 * size_t(C)), o_tpoints = L.take<double>(3 * size_t(P)),
                o_index = L.take<uint32_t>(3 * size_t(M) + P + 2 * size_t(C) + 2),
+               o_order = L.take<uint32_t>(P), o_pstart = L.take<uint32_t>(size_t(P) + 1),
+               o_ocam = L.take<uint32_t>(M), o_opt = L.take<uint32_t>(M), o_opix = L.take<double>(2 * size_t(M)),
+               o_sched = L.take<uint32_t>(p.factored ? M : 0), o_pblk32 = L.take<float>(mixed && p.factored ? 6 * size_t(P) : 0),
                o_tasks = L.take<uint32_t>(max_tasks), o_tobs = L.take<uint32_t>(max_tasks),
                o_ccam = L.take<uint32_t>(max_chunks),
                o_cbeg = L.take<uint32_t>(max_chunks + 1), o_cfirst = L.take<uint32_t>(C + 1),
@@ -433,7 +503,8 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_scal = L.take<double>(size_t(tba::kScalarPartials) * max_task_blocks),
                o_cost = L.take<double>(4 * size_t(max_task_blocks)), o_ticket = L.take<uint32_t>(8),
                o_state = L.take<double>(tba::S_WORDS), o_out = L.take<double>(12 * size_t(C) + 3 * size_t(P) + 27),
-               o_keys = L.take<unsigned long long>(tba::CK_WORDS);
+               o_keys = L.take<unsigned long long>(tba::CK_WORDS),
+               o_diag = L.take<double>((ctl->flags & TBA_FLAG_PRODUCT_ERROR) ? 2 * size_t(m) : 0);
   if (d->capacity < L.bytes) {
     if (d->arena) CUDA_TRY(cudaFree(d->arena));
     d->arena = nullptr;
@@ -457,12 +528,18 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.tposes = D(o_tposes);
   p.tpoints = D(o_tpoints);
   uint32_t* dindex = U32(o_index);
+  // The caller's sections; the point-major ones are replaced by their copies in the engine's point
+  // order once the plan is known (below).
   p.obs_camera = dindex;
   p.obs_point = dindex + M;
   p.point_start = dindex + 2 * size_t(M);
   p.camera_start = p.point_start + P + 1;
   p.camera_obs = p.camera_start + C + 1;
   p.active = p.camera_obs + M;
+  p.obs_point0 = p.obs_point;
+  p.pixels0 = p.pixels;
+  p.sched = p.factored ? U32(o_sched) : nullptr;
+  p.pblk32 = mixed && p.factored ? reinterpret_cast<float*>(a + o_pblk32) : nullptr;
   p.tasks = U32(o_tasks);
   p.task_obs = U32(o_tobs);
   p.chunk_cam = U32(o_ccam);
@@ -474,7 +551,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.pblk = D(o_pblk);
   p.y = D(o_y);
   p.chunk_prod = D(o_cprod);
-  p.F = p.factored ? D(o_F) : nullptr;
+  p.F = p.factored && !mixed ? D(o_F) : nullptr;
   p.F32 = p.factored && mixed ? reinterpret_cast<float*>(a + o_F32) : nullptr;
   p.pw = D(o_pw);
   p.xw = D(o_xw);
@@ -530,7 +607,12 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     up_host(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
     up_host(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
     up_host(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
+    if (!plan.order.empty()) {
+      up_host(U32(o_order), plan.order.data(), sizeof(uint32_t) * P);
+      up_host(U32(o_pstart), plan.pstart.data(), sizeof(uint32_t) * (size_t(P) + 1));
+    }
   }
+  const bool reordered = plannable && !plan.order.empty();
   p.normalize_scale = plan.fixed == 1;
   p.ntasks = ntasks;
   p.nchunks = nchunks;
@@ -571,6 +653,20 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   }
 
   uint32_t launches = 0, lm_done = 0, refinements = 0;
+  // The point-major sections in the engine's point order (after the checks: every offset valid).
+  if (reordered) {
+    const uint32_t* ps0 = p.point_start;
+    const uint32_t* oc0 = p.obs_camera;
+    p.obs_camera = U32(o_ocam);
+    p.obs_point = U32(o_opt);
+    p.pixels = D(o_opix);
+    p.point_start = U32(o_pstart);
+    tba::launch_reorder(p, U32(o_order), ps0, oc0, p.pixels0, s);
+    launches += p.factored ? 2 : 1;
+  } else if (p.factored) {
+    // The caller's order (a problem without a plan never gets here): tasks still need camera order.
+    tba::launch_reorder(p, nullptr, nullptr, nullptr, nullptr, s);
+  }
   // Event pairs around the Schur products; after the solve, only the products that ran PCG steps
   // (the first `steps` of each LM iteration; later ones are guarded no-ops) count.
   std::vector<std::pair<size_t, size_t>> product_events;
@@ -582,17 +678,47 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   launches += 4;
   CUDA_TRY(cudaGetLastError());
   bool lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
-  // The mixed form's FP64 tail: the one-pass product over the FP64 factors (the two-pass recompute
-  // product when the engine keeps no factors).
+  // The mixed form's FP64 tail: the two-pass product, recomputing the FP64 Jacobians (the mixed
+  // form keeps FP32 factors only).
   tba::Params tail = p;
   tail.F32 = nullptr;
+  tail.factored = 0;
   tail.tol_inner = 0;  // the tail stops at the solve's own tolerance
+  double product_error_max = 0, product_error_norm = 0;
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
     tba::launch_point_pass(p, s);
     tba::launch_camera_pass(p, s);
     tba::launch_camera_finish(p, s);
     tba::launch_pcg_init(p, s);
     launches += 4;
+    if (it == 0 && (ctl->flags & TBA_FLAG_PRODUCT_ERROR) && read_word(d, p.state, tba::S_CG_ACTIVE) != 0) {
+      // The solve's own product and the FP64 two-pass product on the first PCG direction.
+      double* own = D(o_diag);
+      double* ref = own + m;
+      tba::Params fp64 = p;
+      fp64.F32 = nullptr;
+      fp64.factored = 0;
+      tba::launch_product(p, s);
+      tba::launch_product_rows(p, own, s);
+      tba::launch_product(fp64, s);
+      tba::launch_product_rows(fp64, ref, s);
+      launches += p.factored ? 5 : 6;
+      CUDA_TRY(cudaGetLastError());
+      std::vector<double> a(m), b(m);
+      CUDA_TRY(cudaMemcpyAsync(a.data(), own, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaMemcpyAsync(b.data(), ref, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaStreamSynchronize(s));
+      double dmax = 0, bmax = 0, d2 = 0, b2 = 0;
+      for (uint32_t j = 0; j < m; j++) {
+        const double e = a[j] - b[j];
+        dmax = std::max(dmax, std::fabs(e));
+        bmax = std::max(bmax, std::fabs(b[j]));
+        d2 += e * e;
+        b2 += b[j] * b[j];
+      }
+      product_error_max = bmax > 0 ? dmax / bmax : dmax;
+      product_error_norm = b2 > 0 ? std::sqrt(d2 / b2) : std::sqrt(d2);
+    }
     // PCG in chunks of guarded iterations; the read after each chunk only ends the loop early.
     uint32_t done = 0, steps_before = 0;
     // `q` selects the product: the engine's own (FP32 factors in the mixed form), or the FP64
@@ -626,17 +752,25 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
       steps_before = steps;
     };
     run_pcg(ctl->max_cg, p, true);
-    // Mixed form: FP64 iterative refinement.  The true residual of the FP32-product solution
-    // restarts the PCG when it is above the tolerance, and the restarted run (with an iteration
-    // budget of its own) uses the FP64 product, which resolves what FP32 factors cannot on badly
-    // conditioned systems.
+    // Mixed form: FP64 iterative refinement.  The true (FP64) residual of the FP32-product solution
+    // restarts the PCG from that solution when it is above the tolerance; a restarted run (with an
+    // iteration budget of its own) uses the FP32 product again and is checked again.  Only a
+    // solution still above the tolerance after kFp32Restarts such runs is finished on the FP64
+    // product, which resolves what FP32 factors cannot on badly conditioned systems.
     if (mixed) {
-      tba::launch_refine(p, s);
-      launches += 4;
-      CUDA_TRY(cudaGetLastError());
-      if (read_word(d, p.state, tba::S_CG_ACTIVE) != 0) {
+      constexpr int kFp32Restarts = 2;
+      for (int round = 0;; round++) {
+        tba::launch_refine(p, s);
+        launches += 4;
+        CUDA_TRY(cudaGetLastError());
+        if (read_word(d, p.state, tba::S_CG_ACTIVE) == 0) break;
         refinements++;
+        if (round < kFp32Restarts) {
+          run_pcg(done + ctl->max_cg, p, true);
+          continue;
+        }
         run_pcg(done + ctl->max_cg, tail, false);
+        break;
       }
     }
     tba::launch_update_cameras(p, s);
@@ -703,6 +837,8 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     report->engine = p.factored ? 0 : 1;
     report->product_blocks = p.factored ? p.prod_blocks : 0;
     report->refinements = uint32_t(refinements);
+    report->product_error_max = product_error_max;
+    report->product_error_norm = product_error_norm;
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
   }
 }
@@ -805,7 +941,8 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
   const size_t factor_size = mixed ? 4 : 8;
   const size_t o_scene = L.take<double>(scene_len), o_index = L.take<uint32_t>(index_len),
                o_out = L.take<double>(output_len), o_tasks = L.take<uint32_t>(tasks.size()),
-               o_desc = L.take<tba::BatchProblem>(count), o_order = L.take<uint32_t>(count),
+               o_desc = L.take<tba::BatchProblem>(count), o_desc64 = L.take<tba::BatchProblem>(mixed ? count : 0),
+               o_order = L.take<uint32_t>(count),
                o_queue = L.take<uint32_t>(4);
   std::vector<size_t> o_tp(count), o_pb(count), o_F(count), o_F64(count);
   uint64_t M_total = 0;
@@ -905,16 +1042,33 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
   up(o_tasks, tasks.data(), tasks.size() * sizeof(uint32_t));
   up(o_desc, desc.data(), desc.size() * sizeof(tba::BatchProblem));
   up(o_order, order.data(), order.size() * sizeof(uint32_t));
+  // A mixed request may also run as the FP64 form (the tuner's policy choice below): the same
+  // problems with their factors in the FP64 region and no FP32 copy.
+  tba::BatchArgs args64 = args;
+  if (mixed) {
+    std::vector<tba::BatchProblem> desc64 = desc;
+    for (tba::BatchProblem& b : desc64) {
+      b.F = b.F64;
+      b.F64 = nullptr;
+    }
+    up(o_desc64, desc64.data(), desc64.size() * sizeof(tba::BatchProblem));
+    args64.problems = reinterpret_cast<const tba::BatchProblem*>(a + o_desc64);
+    args64.tol_inner = bc->cg_tolerance;
+  }
   CUDA_TRY(cudaEventRecord(e1, s));
 
-  auto blocks_of = [&](int shape) {
-    const int per_sm = tba::batch_blocks_per_sm(shape, shared, mixed, smem);
+  auto blocks_of = [&](int shape, bool form_mixed) {
+    const int per_sm = tba::batch_blocks_per_sm(shape, shared, form_mixed, smem);
     return std::min<int>(int(count), per_sm * d->sms);
   };
-  // The launch shape: forced, cached, or tuned now by one timed LM iteration of the whole batch per
-  // shape (the trial launches write only the workspace and the device copy of the results).
+  // The launch shape, and for a mixed request the form: forced, cached, or tuned now by one timed
+  // LM iteration of the whole batch per shape (the trial launches write only the workspace and the
+  // device copy of the results).  A mixed request tries the FP64 form too and keeps it when it is
+  // faster: on small windows the FP32 product saves less than the FP64 refinement of each PCG
+  // solution costs.  The result is the FP64 form's, which the mixed form only approximates.
   double tune_ms = 0;
   int shape = -1;
+  bool run_mixed = mixed;
   if (bc->schedule > 0) {
     shape = int(bc->schedule) - 1;
     if (shape >= tba::kBatchShapes) argument("Invalid GPU BA batch schedule");
@@ -925,40 +1079,46 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
                             std::to_string(lg) + "/" + std::to_string(count);
     auto hit = d->tuned.find(key);
     if (hit != d->tuned.end()) {
-      shape = hit->second;
+      shape = hit->second % tba::kBatchShapes;
+      run_mixed = mixed && hit->second < tba::kBatchShapes;
     } else {
       const auto t0 = std::chrono::steady_clock::now();
       float best = 0;
-      tba::BatchArgs trial = args;
-      trial.iterations = std::min<uint32_t>(args.iterations, 1);
       cudaEvent_t ta = event(d, 4), tb = event(d, 5);
-      for (int k = 0; k < tba::kBatchShapes; k++) {
-        const int blocks = blocks_of(k);
-        if (blocks <= 0) continue;
-        CUDA_TRY(cudaMemsetAsync(trial.queue, 0, sizeof(uint32_t), s));
-        CUDA_TRY(cudaEventRecord(ta, s));
-        CUDA_TRY(tba::launch_batch(k, shared, mixed, trial, blocks, smem, s));
-        CUDA_TRY(cudaEventRecord(tb, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        float ms = 0;
-        CUDA_TRY(cudaEventElapsedTime(&ms, ta, tb));
-        if (shape < 0 || ms < best) {
-          best = ms;
-          shape = k;
+      for (int form = 0; form < (mixed ? 2 : 1); form++) {
+        const bool form_mixed = mixed && form == 0;
+        tba::BatchArgs trial = form_mixed || !mixed ? args : args64;
+        trial.iterations = std::min<uint32_t>(args.iterations, 1);
+        for (int k = 0; k < tba::kBatchShapes; k++) {
+          const int blocks = blocks_of(k, form_mixed);
+          if (blocks <= 0) continue;
+          CUDA_TRY(cudaMemsetAsync(trial.queue, 0, sizeof(uint32_t), s));
+          CUDA_TRY(cudaEventRecord(ta, s));
+          CUDA_TRY(tba::launch_batch(k, shared, form_mixed, trial, blocks, smem, s));
+          CUDA_TRY(cudaEventRecord(tb, s));
+          CUDA_TRY(cudaStreamSynchronize(s));
+          float ms = 0;
+          CUDA_TRY(cudaEventElapsedTime(&ms, ta, tb));
+          if (shape < 0 || ms < best) {
+            best = ms;
+            shape = k;
+            run_mixed = form_mixed;
+          }
         }
       }
       if (shape < 0) throw Fail{TBA_ERROR_INTERNAL, "no launch shape of the batched solver fits the device"};
-      d->tuned[key] = shape;
+      d->tuned[key] = shape + (mixed && !run_mixed ? tba::kBatchShapes : 0);
       tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
   }
-  const int blocks = blocks_of(shape);
+  if (!run_mixed) args = args64;  // (args64 == args for an FP64 request)
+  const int blocks = blocks_of(shape, run_mixed);
   if (blocks <= 0) throw Fail{TBA_ERROR_INTERNAL, "the batched solver's launch shape does not fit the device"};
 
   // One persistent launch, captured once in a CUDA graph and replayed while its arguments stay.
   std::vector<char> key(sizeof args + 3 * sizeof(int) + sizeof(size_t));
   {
-    const int ints[3] = {shape, blocks, int(shared) | (int(mixed) << 1)};
+    const int ints[3] = {shape, blocks, int(shared) | (int(run_mixed) << 1)};
     std::memcpy(key.data(), &args, sizeof args);
     std::memcpy(key.data() + sizeof args, ints, sizeof ints);
     std::memcpy(key.data() + sizeof args + sizeof ints, &smem, sizeof smem);
@@ -973,7 +1133,7 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
     cudaGraph_t graph = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaError_t e1c = cudaMemsetAsync(args.queue, 0, sizeof(uint32_t), s);
-    cudaError_t e2c = e1c == cudaSuccess ? tba::launch_batch(shape, shared, mixed, args, blocks, smem, s) : e1c;
+    cudaError_t e2c = e1c == cudaSuccess ? tba::launch_batch(shape, shared, run_mixed, args, blocks, smem, s) : e1c;
     cudaError_t e3c = cudaStreamEndCapture(s, &graph);
     CUDA_TRY(e2c);
     CUDA_TRY(e3c);
@@ -1027,6 +1187,7 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
     report->blocks = uint32_t(blocks);
     report->graph_replayed = replayed ? 1 : 0;
     report->kernel_launches = 2;
+    report->form = run_mixed ? TBA_PRECISION_MIXED : TBA_PRECISION_FP64;
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
   }
 }
@@ -1149,6 +1310,9 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     CUDA_TRY(cudaStreamSynchronize(s));
   };
   uint32_t cg_total = 0, failed = 0, point_failures = 0;
+  const bool time_products = (vc->flags & TBA_VJP_FLAG_TIME_PRODUCTS) != 0;
+  double product_ms = 0;
+  uint32_t product_launches = 0;
   double last_residual = 0, gnorm_initial = -1, gnorm = 0;
   // One linear solve (H + gauge term) z = rhs by Schur complement and PCG; z lands in x (cameras)
   // and lp (points).  The assembly also measures |F|^2 at the current point.
@@ -1159,12 +1323,25 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     launches += tba::adj_launch_pcg_init(A, s);
     CUDA_TRY(cudaGetLastError());
     uint32_t done = 0;
+    const bool timed = time_products && A.prod_blocks;
     while (done < vc->max_cg) {
       const uint32_t k = std::min<uint32_t>(16, vc->max_cg - done);
-      for (uint32_t j = 0; j < k; j++) launches += tba::adj_launch_pcg_step(A, s);
+      for (uint32_t j = 0; j < k; j++)
+        launches += timed ? tba::adj_launch_pcg_step(A, s, event(d, 8 + 2 * j), event(d, 9 + 2 * j))
+                          : tba::adj_launch_pcg_step(A, s);
       CUDA_TRY(cudaGetLastError());
       done += k;
       read_state();
+      if (timed) {
+        // The chunk's products that ran PCG steps (later launches of a chunk are guarded no-ops).
+        const uint32_t steps = uint32_t(d->pinned[tba::A_STEPS]);
+        for (uint32_t j = 0; j < k && done - k + j < steps; j++) {
+          float ms = 0;
+          CUDA_TRY(cudaEventElapsedTime(&ms, event(d, 8 + 2 * j), event(d, 9 + 2 * j)));
+          product_ms += ms;
+          product_launches++;
+        }
+      }
       if (d->pinned[tba::A_ACTIVE] == 0) break;
     }
     read_state();
@@ -1256,6 +1433,9 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     report->failed = failed;
     report->invalid = uint32_t(invalid);
     report->point_failures = point_failures;
+    report->product_ms = product_ms;
+    report->product_launches = product_launches;
+    report->product_blocks = A.prod_blocks;
     report->kernel_launches = launches;
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
   }
@@ -1274,7 +1454,8 @@ void evaluate_observations(tba_device* d, const tba_observation_control* oc, con
                o_pix = L.take<double>(2 * size_t(M)), o_idx = L.take<uint32_t>(2 * size_t(M)),
                o_off = L.take<uint32_t>(guarded ? size_t(P) + 1 : 0),
                o_flags = L.take<uint32_t>(size_t(M) + (guarded ? P : 0)), o_err = L.take<double>(M),
-               o_part = L.take<double>(2 * ((size_t(M) + 63) / 64)), o_sum = L.take<double>(2);
+               o_part = L.take<double>(2 * ((size_t(M) + 63) / 64)), o_sum = L.take<double>(2),
+               o_tasks = L.take<uint32_t>(guarded ? size_t(P) + 1 : 0);
   if (d->capacity < L.bytes) {
     if (d->arena) CUDA_TRY(cudaFree(d->arena));
     d->arena = nullptr;
@@ -1316,7 +1497,14 @@ void evaluate_observations(tba_device* d, const tba_observation_control* oc, con
   up(o_pts, points, 3 * sizeof(double) * P);
   up(o_pix, pixels, 2 * sizeof(double) * M);
   up(o_idx, indices, 2 * sizeof(uint32_t) * M);
-  if (guarded) up(o_off, offsets, sizeof(uint32_t) * (size_t(P) + 1));
+  if (guarded) {
+    up(o_off, offsets, sizeof(uint32_t) * (size_t(P) + 1));
+    // Warp tasks of whole tracks, built while the copies above run.
+    const std::vector<uint32_t> tasks = build_tasks(offsets, P);
+    p.tasks = reinterpret_cast<uint32_t*>(a + o_tasks);
+    p.ntasks = uint32_t(tasks.size() - 1);
+    up(o_tasks, tasks.data(), sizeof(uint32_t) * tasks.size());
+  }
   CUDA_TRY(cudaEventRecord(e1, s));
   tba::launch_observations(p, s);
   CUDA_TRY(cudaGetLastError());
@@ -1337,7 +1525,7 @@ void evaluate_observations(tba_device* d, const tba_observation_control* oc, con
     report->download_ms = ms;
     report->h2d_bytes = h2d;
     report->d2h_bytes = nflags * sizeof(uint32_t) + 2 * sizeof(double);
-    report->kernel_launches = (M ? 1u : 0u) + (guarded && P ? 1u : 0u) + (M ? 1u : 0u) + 1u;
+    report->kernel_launches = (guarded ? (p.ntasks ? 1u : 0u) : (M ? 1u : 0u)) + (M ? 1u : 0u) + 1u;
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
   }
 }
@@ -1498,7 +1686,7 @@ tba_status tba_bundle_vjp(tba_device* d, const tba_vjp_control* vc, const double
     c.cg_tolerance = 1e-6;
     c.stall_tolerance = 1e-9;
     check_control(&c);
-    if (vc->newton_steps > 50 || vc->max_cg < 1 || vc->max_cg > 100000 || vc->flags != 0 ||
+    if (vc->newton_steps > 50 || vc->max_cg < 1 || vc->max_cg > 100000 || (vc->flags & ~TBA_VJP_FLAG_TIME_PRODUCTS) != 0 ||
         !(std::isfinite(vc->cg_tolerance) && vc->cg_tolerance >= 1e-15 && vc->cg_tolerance <= 1e-2))
       argument("Invalid GPU BA adjoint options");
     if (!scene || !index) argument("Invalid GPU BA arrays: null pointer");
@@ -1731,6 +1919,13 @@ tba_status tba_scene_read(tba_device* d, tba_scene* r, double* poses, double* po
   return TBA_OK;
 }
 
+tba_status tba_device_set_wait_limit(tba_device* d, uint32_t polls) {
+  if (!d) return TBA_ERROR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(d->mu);
+  d->wait_limit = polls;
+  return TBA_OK;
+}
+
 // Rows per slice of an inverse-depth call (2,048 tiles of 128 rows; at most 8 slices a call).
 constexpr uint32_t kIdSliceRows = 1u << 18;
 
@@ -1786,7 +1981,7 @@ tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const doub
                                cudaMemcpyHostToDevice, s));
       CUDA_TRY(cudaEventRecord(ev[1], s));
       CUDA_TRY(tba::launch_linearize_inverse_depth(n, din + 34 * size_t(first), dout + 23 * size_t(first), derr,
-                                                   d->sms, s));
+                                                   d->sms, s, d->wait_limit));
       launched++;
       CUDA_TRY(cudaEventRecord(ev[2], s));
       CUDA_TRY(cudaStreamWaitEvent(down, ev[2], 0));
@@ -1798,7 +1993,9 @@ tba_status tba_linearize_inverse_depth(tba_device* d, uint32_t count, const doub
     CUDA_TRY(cudaMemcpyAsync(&err, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     CUDA_TRY(cudaStreamSynchronize(down));
-    if (err) throw Fail{TBA_ERROR_CUDA, "Inverse-depth linearization: a tile load did not complete"};
+    if (err == 1) throw Fail{TBA_ERROR_CUDA, "Inverse-depth linearization: a tile load did not complete"};
+    if (err) throw Fail{TBA_ERROR_CUDA, "Inverse-depth linearization: a tile load did not complete, and the loads "
+                                        "in flight after it did not land in time"};
     if (report) {
       std::memset(report, 0, sizeof *report);
       // Sums over the slices (the phases of different slices overlap).

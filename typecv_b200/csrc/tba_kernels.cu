@@ -119,9 +119,52 @@ __global__ void k_setup(Params P) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < P.C) P.rlim[k] = radial_limit(P.cams[6 * size_t(k) + 4], P.cams[6 * size_t(k) + 5]);
   if (k < P.M) {
-    const uint32_t i = P.camera_obs[k];
-    P.cm_point[k] = P.obs_point[i];
-    reinterpret_cast<double2*>(P.cm_pixel)[k] = reinterpret_cast<const double2*>(P.pixels)[i];
+    const uint32_t i = P.camera_obs[k];  // an observation of the caller's point-major order
+    P.cm_point[k] = P.obs_point0[i];
+    reinterpret_cast<double2*>(P.cm_pixel)[k] = reinterpret_cast<const double2*>(P.pixels0)[i];
+  }
+}
+
+// The observations in the engine's point order: position q holds the caller's point order[q],
+// whose observations move from ps0[order[q]] in the caller's arrays to point_start[q].  Runs after
+// the structural checks, so every offset is in range.
+__global__ void k_reorder(Params P, const uint32_t* order, const uint32_t* ps0, const uint32_t* oc0,
+                          const double* px0) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P.P) return;
+  const uint32_t p = order[q], from = ps0[p], n = ps0[p + 1] - from, to = P.point_start[q];
+  uint32_t* oc = const_cast<uint32_t*>(P.obs_camera);
+  uint32_t* op = const_cast<uint32_t*>(P.obs_point);
+  double2* px = reinterpret_cast<double2*>(const_cast<double*>(P.pixels));
+  const double2* src = reinterpret_cast<const double2*>(px0);
+  for (uint32_t k = 0; k < n; k++) {
+    oc[to + k] = oc0[from + k];
+    op[to + k] = p;
+    px[to + k] = src[from + k];
+  }
+}
+
+// The camera order of each task of at most 32 observations (the one-pass product's lanes): the
+// task's observations sorted by camera, ties in point-major order.  One warp per task.
+__global__ void __launch_bounds__(256) k_task_order(Params P) {
+  __shared__ uint32_t slot[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* sched = const_cast<uint32_t*>(P.sched);
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + warp; t < P.ntasks; t += warps) {
+    const uint32_t o0 = P.task_obs[t], n = P.task_obs[t + 1] - o0;
+    if (n > uint32_t(kTaskObs)) continue;  // a long point: swept in rounds, no camera order
+    const bool valid = uint32_t(lane) < n;
+    const uint32_t cam = valid ? P.obs_camera[o0 + lane] : 0u;
+    const uint32_t key = valid ? (cam << 5) | uint32_t(lane) : 0x80000000u | uint32_t(lane);  // cam < 2^16
+    uint32_t rank = 0;
+    for (int k = 0; k < 32; k++) rank += __shfl_sync(kFull, key, k) < key;
+    slot[warp][rank] = uint32_t(lane);  // camera-order lane `rank` takes offset `lane`
+    __syncwarp();
+    const uint32_t j = slot[warp][lane];
+    const uint32_t cj = __shfl_sync(kFull, cam, j);
+    if (valid) sched[o0 + lane] = cj | (j << 16) | (rank << 21);
+    __syncwarp();
   }
 }
 
@@ -194,8 +237,9 @@ __device__ inline void point_obs(const Params& P, uint32_t i, uint32_t pt, doubl
     f[10] = g.jf[0];
     f[11] = g.jf[1];
     const size_t stride = P.Mpad;
-    // FP64 factors always; the mixed form's PCG reads an FP32 copy.
-    for (int k = 0; k < kFactors; k++) P.F[k * stride + i] = f[k];
+    // FP64 factors in the FP64 form, FP32 factors in the mixed form.
+    if (P.F)
+      for (int k = 0; k < kFactors; k++) P.F[k * stride + i] = f[k];
     if (P.F32)
       for (int k = 0; k < kFactors; k++) P.F32[k * stride + i] = float(f[k]);
   }
@@ -226,14 +270,19 @@ __device__ inline void point_finish(const Params& P, uint32_t pt, const double (
   double inv[6];
   const bool ok = v[12] == 0 && inverse3_spd(V, inv);
   double2* blk = reinterpret_cast<double2*>(P.pblk + 12 * size_t(pt));
+  float2* blk32 = P.pblk32 ? reinterpret_cast<float2*>(P.pblk32 + 6 * size_t(pt)) : nullptr;
   if (!ok) {
     P.state[S_POINT_FAILED] = 1;
     for (int k = 0; k < 6; k++) blk[k] = make_double2(0, 0);
+    if (blk32)
+      for (int k = 0; k < 3; k++) blk32[k] = make_float2(0, 0);
     return;
   }
   blk[0] = make_double2(inv[0], inv[1]);
   blk[1] = make_double2(inv[2], inv[3]);
   blk[2] = make_double2(inv[4], inv[5]);
+  if (blk32)  // the FP32 product's copy of the FP64 inverse
+    for (int k = 0; k < 3; k++) blk32[k] = make_float2(float(inv[2 * k]), float(inv[2 * k + 1]));
   blk[3] = make_double2(v[6], v[7]);
   blk[4] = make_double2(v[8], 0);
   if (SHARED) {
@@ -256,6 +305,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
   uint32_t tb, te;
   block_tasks(P, tb, te);
   for (uint32_t t = tb + warp; t < te; t += nwarps) {
+    // Positions p0 <= q < p1 of the engine's point order; a lane's point id comes from obs_point.
     const uint32_t p0 = P.tasks[t], p1 = P.tasks[t + 1];
     const uint32_t o0 = P.point_start[p0], n = P.point_start[p1] - o0;
     if (n <= uint32_t(kTaskObs)) {
@@ -264,7 +314,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
       uint32_t pt = 0;
       if (uint32_t(lane) < n) {
         pt = P.obs_point[o0 + lane];
-        seg = int(pt - p0);
+        seg = int(pt);
         point_obs<SHARED>(P, o0 + lane, pt, fscale, v, sc[0], sc[1]);
       }
       const Runs runs = lane_runs(seg, lane);
@@ -272,16 +322,17 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
       if (uint32_t(lane) < n && run_tail(runs, lane))
         point_finish<SHARED>(P, pt, v, lambda, sc[2], sc[3]);
     } else {
+      const uint32_t pt = P.obs_point[o0];
       double v[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (uint32_t base = 0; base < n; base += kTaskObs) {
         if (base + lane < n) {
           double u[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-          point_obs<SHARED>(P, o0 + base + lane, p0, fscale, u, sc[0], sc[1]);
+          point_obs<SHARED>(P, o0 + base + lane, pt, fscale, u, sc[0], sc[1]);
           for (int k = 0; k < 13; k++) v[k] += u[k];
         }
       }
       warp_allsum(v);
-      if (lane == 0) point_finish<SHARED>(P, p0, v, lambda, sc[2], sc[3]);
+      if (lane == 0) point_finish<SHARED>(P, pt, v, lambda, sc[2], sc[3]);
     }
   }
   block_sum(sc, red);
@@ -543,24 +594,25 @@ __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_schur_p
       uint32_t pt = 0;
       if (uint32_t(lane) < n) {
         pt = P.obs_point[o0 + lane];
-        seg = int(pt - p0);
+        seg = int(pt);
         schur_point_obs<SHARED>(P, o0 + lane, pt, fscale, pf, s);
       }
       const Runs runs = lane_runs(seg, lane);
       run_scan(s, runs);
       if (uint32_t(lane) < n && run_tail(runs, lane)) schur_point_finish(P, pt, s);
     } else {
+      const uint32_t pt = P.obs_point[o0];
       double s[3] = {0, 0, 0};
       for (uint32_t base = 0; base < n; base += kTaskObs)
         if (base + lane < n) {
           double u[3];
-          schur_point_obs<SHARED>(P, o0 + base + lane, p0, fscale, pf, u);
+          schur_point_obs<SHARED>(P, o0 + base + lane, pt, fscale, pf, u);
           s[0] += u[0];
           s[1] += u[1];
           s[2] += u[2];
         }
       warp_allsum(s);
-      if (lane == 0) schur_point_finish(P, p0, s);
+      if (lane == 0) schur_point_finish(P, pt, s);
     }
   }
 }
@@ -619,7 +671,48 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // pair k of camera c at k * C + c, read as one 16- or 8-byte word): the lanes of a warp touch random
 // cameras, and with camera-major records of 6 words the 8-byte accesses of a warp would fall on only
 // 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over all of them.
-template <bool SHARED, typename T, bool STAGED>
+// V_p^-1 (6 unique values) in the product's arithmetic type: the FP32 copy when the FP32 product
+// has one, else the FP64 block.
+template <typename T>
+__device__ inline void load_point_inverse(const Params& P, uint32_t pt, T (&vb)[6]) {
+  if constexpr (sizeof(T) == 4) {
+    if (P.pblk32) {
+      const float2* b = reinterpret_cast<const float2*>(P.pblk32 + 6 * size_t(pt));
+      for (int k = 0; k < 3; k++) {
+        const float2 d = b[k];
+        vb[2 * k] = d.x;
+        vb[2 * k + 1] = d.y;
+      }
+      return;
+    }
+  }
+  double d[6];
+  load6(P.pblk + 12 * size_t(pt), d);
+  for (int k = 0; k < 6; k++) vb[k] = T(d[k]);
+}
+
+// W_i^T x in the factors' arithmetic type, from the camera's step in world axes xw and the focal
+// step xf (a bearing has no translation rows).
+template <typename T>
+__device__ inline void factor_wt_t(const Factors<T>& f, const T (&xw)[6], T xf, bool dir, bool shared, T t[3]) {
+  T m0 = xw[1] * f.q[2] - xw[2] * f.q[1], m1 = xw[2] * f.q[0] - xw[0] * f.q[2], m2 = xw[0] * f.q[1] - xw[1] * f.q[0];
+  if (!dir) {
+    m0 += xw[3];
+    m1 += xw[4];
+    m2 += xw[5];
+  }
+  T au = f.ju[0] * m0 + f.ju[1] * m1 + f.ju[2] * m2;
+  T av = f.jv[0] * m0 + f.jv[1] * m1 + f.jv[2] * m2;
+  if (shared) {
+    au += f.jf[0] * xf;
+    av += f.jf[1] * xf;
+  }
+  au *= f.w;
+  av *= f.w;
+  for (int k = 0; k < 3; k++) t[k] = au * f.ju[k] + av * f.jv[k];
+}
+
+template <bool SHARED, typename T, typename A, bool STAGED>
 __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 : kStagedThreads) : kProductThreads,
                                   STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double4 product_smem[];
@@ -627,12 +720,13 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
   // It runs while the PCG is active, or, with P.refine, on the mixed form's refinement of x.
   if (P.state[S_CG_ACTIVE] == 0 && !(P.refine && P.state[S_REFINE] != 0)) return;
   const uint32_t m = P.m, C = P.C;
-  // The camera sums (6C values of T: FP64 sums for FP64 factors, FP32 sums of a block's share for
-  // FP32 factors), then the staged direction: three arrays of C pairs (pair k of each camera's 6).
-  T* acc = reinterpret_cast<T*>(product_smem);
+  // The camera sums (6C values of A: FP64 for FP64 factors; for FP32 factors FP64 when they fit
+  // beside the staged direction, so that a warp's FP32 run sums accumulate in FP64, else FP32),
+  // then the staged direction: three arrays of C pairs of T (pair k of each camera's 6).
+  A* acc = reinterpret_cast<A*>(product_smem);
   using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-  T2* pws = reinterpret_cast<T2*>(reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, sizeof(T)));
-  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) acc[j] = T(0);
+  T2* pws = reinterpret_cast<T2*>(reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, sizeof(A)));
+  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) acc[j] = A(0);
   if (threadIdx.x == 0) focal_acc = 0;
   if (STAGED)
     for (uint32_t j = threadIdx.x; j < 3 * C; j += blockDim.x) {
@@ -656,55 +750,80 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
       e_next = P.task_obs[t + nwarps + 1];
     }
     if (n <= uint32_t(kTaskObs)) {
-      // One observation per lane.  Every load the lane needs is issued before any arithmetic: its
-      // camera and point index, its factors, its point's V_p^-1 and its camera's direction.
+      // Two lane orders over the task's n observations (offsets 0..n-1, point-major):
+      //  * point order: lane l holds offset l (its point pq), for the point sums
+      //    y_p = V_p^-1 sum_i W_i^T p;
+      //  * camera order: lane l takes offset j (camera c), the task's observations sorted by camera,
+      //    for the factors, the direction and the camera sums, which then reduce over runs of
+      //    adjacent lanes with one shared-memory atomic per camera.
+      // sched gives each lane its camera-order offset and camera, and the camera-order lane (inv)
+      // of its point-order offset.  Lanes >= n idle in both orders (j = inv = lane).  Every load a
+      // lane needs is issued before any arithmetic.
       const bool valid = uint32_t(lane) < n;
-      const uint32_t i = o0 + (valid ? lane : 0);
-      const uint32_t c = P.obs_camera[i], pt = P.obs_point[i];
+      const uint32_t w = valid ? __ldg(P.sched + o0 + lane) : (uint32_t(lane) << 16) | (uint32_t(lane) << 21);
+      const uint32_t pq = valid ? __ldg(P.obs_point + o0 + lane) : 0u;
+      const uint32_t c = valid ? (w & 0xffffu) : 0u, j = (w >> 16) & 31u, inv = (w >> 21) & 31u;
       Factors<T> f;
-      load_factors(FT, stride, i, f);
-      double vb[6], xw[6];
-      load6(P.pblk + 12 * size_t(pt), vb);
-      if (STAGED)
+      load_factors(FT, stride, o0 + (valid ? j : 0u), f);
+      // Point order: the last lane of each point loads its V_p^-1.
+      const uint32_t pn = __shfl_down_sync(kFull, pq, 1);
+      const bool ptail = valid && (uint32_t(lane) + 1 == n || pn != pq);
+      T vb[6] = {0, 0, 0, 0, 0, 0};
+      if (ptail) load_point_inverse(P, pq, vb);
+      T xw[6];
+      if (STAGED) {
         for (int k = 0; k < 3; k++) {
-          const T2 v = pws[k * C + c];
-          xw[2 * k] = double(v.x);
-          xw[2 * k + 1] = double(v.y);
+          const T2 d = pws[k * C + c];
+          xw[2 * k] = d.x;
+          xw[2 * k + 1] = d.y;
         }
-      else
-        load6(P.pw + 6 * size_t(c), xw);
-      // A fixed camera's direction is zero, so its observations add nothing on the camera side;
-      // their scatter lands in the fixed camera's rows, which k_product_columns discards.
-      const uint32_t p0 = __shfl_sync(kFull, pt, 0);
-      const int seg = valid ? int(pt - p0) : -1 - lane;
-      double s[3] = {0, 0, 0};
-      if (valid) factor_wt(f, xw, pf, true, directional(P, pt), SHARED, s);
-      const Runs runs = lane_runs(seg, lane);
-      run_scan(s, runs);
-      const bool tail = valid && run_tail(runs, lane);
-      double y[3] = {0, 0, 0};
-      if (tail) {
-        y[0] = vb[0] * s[0] + vb[1] * s[1] + vb[2] * s[2];
-        y[1] = vb[1] * s[0] + vb[3] * s[1] + vb[4] * s[2];
-        y[2] = vb[2] * s[0] + vb[4] * s[1] + vb[5] * s[2];
+      } else {
+        double d[6];
+        load6(P.pw + 6 * size_t(c), d);
+        for (int k = 0; k < 6; k++) xw[k] = T(d[k]);
       }
-      const unsigned tails = __ballot_sync(kFull, tail);
-      const int src = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
-      for (int j = 0; j < 3; j++) y[j] = __shfl_sync(kFull, y[j], src);
-      if (!valid) continue;
-      const T y0 = T(y[0]), y1 = T(y[1]), y2 = T(y[2]);
-      const T gu = f.w * (f.ju[0] * y0 + f.ju[1] * y1 + f.ju[2] * y2);
-      const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
-      if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
-      const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      T* ac = acc + c;
-      atomicAdd(ac, -(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + C, -(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2 * C, -(f.q[0] * h1 - f.q[1] * h0));
-      if (!directional(P, pt)) {
-        atomicAdd(ac + 3 * C, -h0);
-        atomicAdd(ac + 4 * C, -h1);
-        atomicAdd(ac + 5 * C, -h2);
+      // A fixed camera's direction is zero, so its observations add nothing on the point side; their
+      // camera sums land in the fixed camera's rows, which k_product_columns discards.
+      const bool dir = directional(P, __shfl_sync(kFull, pq, j));
+      T sc[3] = {0, 0, 0};
+      if (valid) factor_wt_t(f, xw, T(pf), dir, SHARED, sc);
+      T sq[3];
+      for (int k = 0; k < 3; k++) sq[k] = __shfl_sync(kFull, sc[k], inv);
+      const Runs pr = lane_runs(valid ? int(pq) : -1 - lane, lane);
+      run_scan(sq, pr);
+      T yq[3] = {0, 0, 0};
+      if (ptail) {
+        yq[0] = vb[0] * sq[0] + vb[1] * sq[1] + vb[2] * sq[2];
+        yq[1] = vb[1] * sq[0] + vb[3] * sq[1] + vb[4] * sq[2];
+        yq[2] = vb[2] * sq[0] + vb[4] * sq[1] + vb[5] * sq[2];
+      }
+      const unsigned tails = __ballot_sync(kFull, ptail);
+      const int srcq = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
+      // Camera order again: each lane takes y_p of its observation's point.
+      const int src = __shfl_sync(kFull, srcq, j);
+      T y[3];
+      for (int k = 0; k < 3; k++) y[k] = __shfl_sync(kFull, yq[k], src);
+      // -W_i y_p in world axes (rotation rows q~ x h, translation rows h), summed per camera run.
+      T v[6] = {0, 0, 0, 0, 0, 0};
+      if (valid) {
+        const T gu = f.w * (f.ju[0] * y[0] + f.ju[1] * y[1] + f.ju[2] * y[2]);
+        const T gv = f.w * (f.jv[0] * y[0] + f.jv[1] * y[1] + f.jv[2] * y[2]);
+        if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
+        const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
+        v[0] = -(f.q[1] * h2 - f.q[2] * h1);
+        v[1] = -(f.q[2] * h0 - f.q[0] * h2);
+        v[2] = -(f.q[0] * h1 - f.q[1] * h0);
+        if (!dir) {
+          v[3] = -h0;
+          v[4] = -h1;
+          v[5] = -h2;
+        }
+      }
+      const Runs cr = lane_runs(valid ? int(c) : -1 - lane, lane);
+      run_scan(v, cr);
+      if (valid && run_tail(cr, lane)) {
+        A* ac = acc + c;
+        for (int k = 0; k < 6; k++) atomicAdd(ac + k * C, A(v[k]));
       }
       continue;
     }
@@ -751,14 +870,14 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
       const T gv = f.w * (f.jv[0] * y0 + f.jv[1] * y1 + f.jv[2] * y2);
       if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
       const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-      T* ac = acc + c;
-      atomicAdd(ac, -(f.q[1] * h2 - f.q[2] * h1));
-      atomicAdd(ac + C, -(f.q[2] * h0 - f.q[0] * h2));
-      atomicAdd(ac + 2 * C, -(f.q[0] * h1 - f.q[1] * h0));
+      A* ac = acc + c;
+      atomicAdd(ac, A(-(f.q[1] * h2 - f.q[2] * h1)));
+      atomicAdd(ac + C, A(-(f.q[2] * h0 - f.q[0] * h2)));
+      atomicAdd(ac + 2 * C, A(-(f.q[0] * h1 - f.q[1] * h0)));
       if (!directional(P, p0)) {
-        atomicAdd(ac + 3 * C, -h0);
-        atomicAdd(ac + 4 * C, -h1);
-        atomicAdd(ac + 5 * C, -h2);
+        atomicAdd(ac + 3 * C, A(-h0));
+        atomicAdd(ac + 4 * C, A(-h1));
+        atomicAdd(ac + 5 * C, A(-h2));
       }
     }
   }
@@ -1001,11 +1120,45 @@ __global__ void k_pcg_direction(Params P) {
   }
 }
 
+// ---- Diagnostics: S p of one product, every row, into `out` --------------------------------------
+//
+// `onepass`: from the one-pass product's partial rows (which hold -sum_i W_i y_p), else from the
+// two-pass product's chunk sums (+sum_i W_i y_p); then U_c p_c, the focal couplings and the focal
+// row, as k_product_columns and k_product_reduce form them.  Writes no state.
+__global__ void __launch_bounds__(256) k_product_rows(Params P, int onepass, double* out) {
+  const uint32_t n = 6 * P.C, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) {
+    const uint32_t c = j / 6, r = j % 6;
+    double sum = 0;
+    if (onepass) {
+      if (P.active[c] != 0)
+        for (uint32_t b = 0; b < P.prod_blocks; b++) sum += P.acc_part[size_t(b) * P.m + j];
+    } else {
+      for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum -= P.chunk_prod[8 * size_t(ch) + r];
+    }
+    const double* U = P.camU + 21 * size_t(c);
+    const double* pc = P.p + 6 * size_t(c);
+    double sp = sum;
+    for (int k = 0; k < 6; k++) sp += U[sym6(r, k)] * pc[k];
+    if (P.shared) sp += P.camHcf[j] * P.p[P.m - 1];
+    out[j] = sp;
+  } else if (j == n && P.shared) {
+    double sp = P.state[S_FOCAL_DIAG] * P.p[n];
+    for (uint32_t k = 0; k < n; k++) sp += P.camHcf[k] * P.p[k];
+    if (onepass)
+      for (uint32_t b = 0; b < P.prod_blocks; b++) sp += P.acc_part[size_t(b) * P.m + n];
+    else
+      for (uint32_t ch = 0; ch < P.nchunks; ch++) sp -= P.chunk_prod[8 * size_t(ch) + 6];
+    out[n] = sp;
+  }
+}
+
 // ---- Mixed form: FP64 iterative refinement of the PCG solution ----------------------------------
 //
 // After the PCG ran on the FP32-factor product, k_refine_begin marks the refinement, an FP64 product
-// evaluates S x (launched with p := x: one pass over the FP64 factors, or the two-pass recompute
-// product when the engine keeps no factors), and k_refine forms the true residual
+// evaluates S x (launched with p := x: the two-pass product, which recomputes the FP64 Jacobians
+// from the poses, points and pixels, since the mixed form stores FP32 factors only; one pass over
+// stored FP64 factors where an engine keeps them), and k_refine forms the true residual
 // r = b - S x, z = M^-1 r, p = z, rho and r.r.  Its last block adds the focal row and either accepts
 // x (r.r within the tolerance: the PCG stays finished) or restarts the PCG from x with this r.
 
@@ -1036,7 +1189,7 @@ __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
     // sum_i W_i y_p of the camera: the column sum of the one-pass product's partial rows (which hold
     // its negative; a fixed camera's rows are discarded), or the two-pass product's chunk sums.
     double sum = 0;
-    if (P.factored) {
+    if (P.factored && P.F) {
       if (P.active[c] != 0)
         for (uint32_t b = 0; b < P.prod_blocks; b++) sum -= P.acc_part[size_t(b) * P.m + row];
     } else {
@@ -1056,7 +1209,7 @@ __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
     rs[threadIdx.x] = rr;
   }
   if (P.shared) {
-    if (P.factored)
+    if (P.factored && P.F)
       for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < P.prod_blocks; b += gridDim.x * blockDim.x)
         v[3] -= P.acc_part[size_t(b) * P.m + (P.m - 1)];
     else
@@ -1211,6 +1364,14 @@ __device__ inline void update_wt(const Params& P, uint32_t i, uint32_t c, uint32
     factor_wt(f, xw, xf, P.active[c] != 0, directional(P, pt), shared, t);
     return;
   }
+  if (P.factored && P.F32) {  // mixed form: the back-substitution's W_i^T x in FP32
+    Factors<float> f;
+    load_factors(static_cast<const float*>(P.F32), P.Mpad, i, f);
+    double xw[6];
+    load6(P.xw + 6 * size_t(c), xw);
+    factor_wt(f, xw, xf, P.active[c] != 0, directional(P, pt), shared, t);
+    return;
+  }
   double pose[12], xc[6];
   Geo g;
   if (observe(P, i, c, pt, fscale, pose, g)) {
@@ -1282,7 +1443,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_update_
       uint32_t pt = 0;
       if (valid) {
         pt = P.obs_point[i];
-        seg = int(pt - p0);
+        seg = int(pt);
         update_wt(P, i, P.obs_camera[i], pt, fscale, xf, SHARED, s);
       }
       const Runs runs = lane_runs(seg, lane);
@@ -1295,7 +1456,7 @@ __global__ void __launch_bounds__(kPointThreads, TBA_SCHUR_MIN_BLOCKS) k_update_
       for (int j = 0; j < 3; j++) X[j] = __shfl_sync(kFull, X[j], src);
       if (valid) candidate_obs(P, i, pt, X, fscale_trial, cs[0], cs[1]);
     } else {
-      const uint32_t pt = p0;
+      const uint32_t pt = P.obs_point[o0];
       double s[3] = {0, 0, 0};
       for (uint32_t base = 0; base < n; base += kTaskObs)
         if (base + lane < n) {
@@ -1394,50 +1555,84 @@ uint32_t product_finish_blocks(const Params& p) {
 
 uint32_t product_max_unknowns() { return uint32_t(kStagedSmemLimit / sizeof(double)) - 64; }
 
+// Bytes of a camera sum: FP64, except with FP32 factors when FP64 sums and the staged FP32
+// direction do not fit one block together.
+size_t product_sum_word(const Params& p) {
+  if (!p.F32) return sizeof(double);
+  return product_sums_bytes(p.C, sizeof(double)) + 6 * size_t(p.C) * sizeof(float) <= size_t(kStagedSmemLimit)
+             ? sizeof(double)
+             : sizeof(float);
+}
+
 // The direction is staged in shared memory when the camera sums and it fit one block.
 bool product_staged(const Params& p) {
   const size_t word = p.F32 ? sizeof(float) : sizeof(double);
-  return product_sums_bytes(p.C, word) + 6 * size_t(p.C) * word <= size_t(kStagedSmemLimit);
+  return product_sums_bytes(p.C, product_sum_word(p)) + 6 * size_t(p.C) * word <= size_t(kStagedSmemLimit);
 }
 
 size_t product_smem_bytes(const Params& p) {
   const size_t word = p.F32 ? sizeof(float) : sizeof(double);
-  return product_sums_bytes(p.C, word) + (product_staged(p) ? 6 * size_t(p.C) * word : 0);
+  return product_sums_bytes(p.C, product_sum_word(p)) + (product_staged(p) ? 6 * size_t(p.C) * word : 0);
 }
 
 int product_threads(const Params& p) {
   return product_staged(p) ? (p.F32 ? kStagedThreadsF32 : kStagedThreads) : kProductThreads;
 }
 
+namespace {
+
+// The product kernel of a solve: focal route, factor type, sum type and staging.
+template <bool SHARED>
+const void* product_kernel_of(const Params& p) {
+  const bool st = product_staged(p);
+  if (!p.F32)
+    return st ? reinterpret_cast<const void*>(k_product_f<SHARED, double, double, true>)
+              : reinterpret_cast<const void*>(k_product_f<SHARED, double, double, false>);
+  if (product_sum_word(p) == sizeof(double)) return reinterpret_cast<const void*>(k_product_f<SHARED, float, double, true>);
+  return st ? reinterpret_cast<const void*>(k_product_f<SHARED, float, float, true>)
+            : reinterpret_cast<const void*>(k_product_f<SHARED, float, float, false>);
+}
+
+const void* product_kernel(const Params& p) { return p.shared ? product_kernel_of<true>(p) : product_kernel_of<false>(p); }
+
+}  // namespace
+
 cudaError_t configure_kernels() {
   const int bytes = kStagedSmemLimit;  // the products also hold a few static bytes
-  cudaError_t e = cudaSuccess;
-  auto set = [&](const void* f) {
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const void* kernels[] = {
+      reinterpret_cast<const void*>(k_product_f<false, double, double, false>),
+      reinterpret_cast<const void*>(k_product_f<true, double, double, false>),
+      reinterpret_cast<const void*>(k_product_f<false, double, double, true>),
+      reinterpret_cast<const void*>(k_product_f<true, double, double, true>),
+      reinterpret_cast<const void*>(k_product_f<false, float, float, false>),
+      reinterpret_cast<const void*>(k_product_f<true, float, float, false>),
+      reinterpret_cast<const void*>(k_product_f<false, float, float, true>),
+      reinterpret_cast<const void*>(k_product_f<true, float, float, true>),
+      reinterpret_cast<const void*>(k_product_f<false, float, double, true>),
+      reinterpret_cast<const void*>(k_product_f<true, float, double, true>),
   };
-  set(reinterpret_cast<const void*>(k_product_f<false, double, false>));
-  set(reinterpret_cast<const void*>(k_product_f<true, double, false>));
-  set(reinterpret_cast<const void*>(k_product_f<false, float, false>));
-  set(reinterpret_cast<const void*>(k_product_f<true, float, false>));
-  set(reinterpret_cast<const void*>(k_product_f<false, double, true>));
-  set(reinterpret_cast<const void*>(k_product_f<true, double, true>));
-  set(reinterpret_cast<const void*>(k_product_f<false, float, true>));
-  set(reinterpret_cast<const void*>(k_product_f<true, float, true>));
-  return e;
+  for (const void* f : kernels) {
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 int product_blocks_per_sm(const Params& p) {
   int n = 0;
-  const bool st = product_staged(p);
-  const void* f = p.F32 ? (st ? reinterpret_cast<const void*>(k_product_f<true, float, true>)
-                              : reinterpret_cast<const void*>(k_product_f<true, float, false>))
-                        : (st ? reinterpret_cast<const void*>(k_product_f<true, double, true>)
-                              : reinterpret_cast<const void*>(k_product_f<true, double, false>));
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, product_threads(p), product_smem_bytes(p)) != cudaSuccess)
+  Params q = p;
+  q.shared = 1;  // both focal routes have the same resources
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, product_kernel(q), product_threads(p), product_smem_bytes(p)) !=
+      cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
 }
 
+void launch_reorder(const Params& p, const uint32_t* order, const uint32_t* ps0, const uint32_t* oc0,
+                    const double* px0, cudaStream_t s) {
+  if (p.P && order) k_reorder<<<(p.P + 255) / 256, 256, 0, s>>>(p, order, ps0, oc0, px0);
+  if (p.factored && p.ntasks) k_task_order<<<(p.ntasks + 7) / 8, 256, 0, s>>>(p);
+}
 void launch_initialize(const Params& p, cudaStream_t s) {
   k_initialize<<<1, 1, 0, s>>>(p);
   const uint32_t n = p.M > p.C ? p.M : p.C;
@@ -1454,23 +1649,9 @@ void launch_camera_finish(const Params& p, cudaStream_t s) { k_camera_finish<<<(
 void launch_pcg_init(const Params& p, cudaStream_t s) { k_pcg_init<<<1, 1024, 0, s>>>(p); }
 void launch_product(const Params& p, cudaStream_t s) {
   if (p.factored) {
-    const size_t smem = product_smem_bytes(p);
-    const int nt = product_threads(p);
-    if (product_staged(p)) {
-      if (p.F32) {
-        if (p.shared) k_product_f<true, float, true><<<p.prod_blocks, nt, smem, s>>>(p);
-        else k_product_f<false, float, true><<<p.prod_blocks, nt, smem, s>>>(p);
-      } else {
-        if (p.shared) k_product_f<true, double, true><<<p.prod_blocks, nt, smem, s>>>(p);
-        else k_product_f<false, double, true><<<p.prod_blocks, nt, smem, s>>>(p);
-      }
-    } else if (p.F32) {
-      if (p.shared) k_product_f<true, float, false><<<p.prod_blocks, nt, smem, s>>>(p);
-      else k_product_f<false, float, false><<<p.prod_blocks, nt, smem, s>>>(p);
-    } else {
-      if (p.shared) k_product_f<true, double, false><<<p.prod_blocks, nt, smem, s>>>(p);
-      else k_product_f<false, double, false><<<p.prod_blocks, nt, smem, s>>>(p);
-    }
+    Params q = p;
+    void* args[] = {&q};
+    cudaLaunchKernel(product_kernel(p), dim3(p.prod_blocks), dim3(product_threads(p)), args, product_smem_bytes(p), s);
     return;
   }
   if (p.shared) {
@@ -1498,12 +1679,12 @@ void launch_refine(const Params& p, cudaStream_t s) {
   Params q = p;
   q.refine = 1;
   q.p = p.x;
-  if (p.factored) {
-    // S x in one pass over the FP64 factors (kept beside the FP32 ones).
+  if (p.factored && p.F) {
+    // S x in one pass over stored FP64 factors.
     q.F32 = nullptr;
     k_refine_direction<<<(p.C + 255) / 256, 256, 0, s>>>(q);
     launch_product(q, s);
-  } else if (p.shared) {
+  } else if (p.shared) {  // S x by the two-pass product, recomputing the FP64 Jacobians
     k_schur_points<true><<<p.task_blocks, kPointThreads, 0, s>>>(q);
     k_schur_cameras<true><<<p.nchunks, kCameraThreads, 0, s>>>(q);
   } else {
@@ -1511,6 +1692,9 @@ void launch_refine(const Params& p, cudaStream_t s) {
     k_schur_cameras<false><<<p.nchunks, kCameraThreads, 0, s>>>(q);
   }
   k_refine<<<(6 * p.C + kUpdateRows - 1) / kUpdateRows, kUpdateThreads, 0, s>>>(p);
+}
+void launch_product_rows(const Params& p, double* out, cudaStream_t s) {
+  k_product_rows<<<(p.m + 255) / 256, 256, 0, s>>>(p, p.factored ? 1 : 0, out);
 }
 void launch_update_cameras(const Params& p, cudaStream_t s) { k_update_cameras<<<1, 256, 0, s>>>(p); }
 void launch_update_points(const Params& p, cudaStream_t s) {

@@ -17,6 +17,12 @@
 // so the scratch bounds the problem: at most kMaxTiles tiles.  A second one-block kernel sums the
 // tile partials in a fixed order into the caller's result.  Nothing is allocated: no cudaMalloc,
 // no cudaFree, no library routine that allocates.
+//
+// Caller buffers are checked before any launch: each of scene, index and result must be device
+// memory of the current device (cudaPointerGetAttributes), and the allocation it lies in must hold
+// the length the caller states (the driver's cuMemGetAddressRange), so that a host pointer or a
+// buffer shorter than the control implies is refused instead of faulting the caller's context.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -105,8 +111,20 @@ __global__ void __launch_bounds__(kThreads) k_tile_finish(const double* partials
   }
 }
 
+// The scratch's device address, per device ordinal, with the context it was looked up in: a caller
+// that resets the device (cudaDeviceReset) or binds another context gets a fresh look-up.
+struct Scratch {
+  CUcontext context = nullptr;
+  double* address = nullptr;
+};
 std::mutex g_setup;
-double* g_scratch[kMaxDevices] = {};  // device address of g_tile_partials, per device ordinal
+Scratch g_scratch[kMaxDevices];
+
+// Driver calls reached through the runtime's entry-point table (no link against libcuda).
+using GetAddressRange = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+using GetCurrentContext = CUresult (*)(CUcontext*);
+GetAddressRange g_range = nullptr;
+GetCurrentContext g_context = nullptr;
 
 void say(char* message, size_t len, const char* text) {
   if (message && len) {
@@ -115,10 +133,69 @@ void say(char* message, size_t len, const char* text) {
   }
 }
 
+bool driver_calls(char* message, size_t len) {
+  if (g_range && g_context) return true;
+  void* range = nullptr;
+  void* context = nullptr;
+  cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &range, cudaEnableDefault, &q1) != cudaSuccess ||
+      cudaGetDriverEntryPoint("cuCtxGetCurrent", &context, cudaEnableDefault, &q2) != cudaSuccess ||
+      q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !range || !context) {
+    cudaGetLastError();
+    say(message, len, "tba_scene_cost_noalloc: the CUDA driver does not provide cuMemGetAddressRange/cuCtxGetCurrent");
+    return false;
+  }
+  g_range = reinterpret_cast<GetAddressRange>(range);
+  g_context = reinterpret_cast<GetCurrentContext>(context);
+  return true;
+}
+
+// True when `p` is device (or managed) memory of device `dev` whose allocation holds `bytes` from
+// `p` on; otherwise the message says why.  Nothing here touches the memory.
+bool device_buffer(const void* p, size_t bytes, int dev, const char* name, char* message, size_t len) {
+  char text[256];
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    std::snprintf(text, sizeof text, "tba_scene_cost_noalloc: %s is not a pointer CUDA knows", name);
+    say(message, len, text);
+    return false;
+  }
+  if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) {
+    std::snprintf(text, sizeof text, "tba_scene_cost_noalloc: %s is %s memory, not device memory", name,
+                  attr.type == cudaMemoryTypeHost ? "page-locked host" : "host");
+    say(message, len, text);
+    return false;
+  }
+  if (attr.type == cudaMemoryTypeDevice && attr.device != dev) {
+    std::snprintf(text, sizeof text, "tba_scene_cost_noalloc: %s is memory of device %d, not of the current device %d",
+                  name, attr.device, dev);
+    say(message, len, text);
+    return false;
+  }
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  const CUdeviceptr at = reinterpret_cast<CUdeviceptr>(p);
+  if (g_range(&base, &size, at) != CUDA_SUCCESS) {
+    std::snprintf(text, sizeof text, "tba_scene_cost_noalloc: %s lies in no device allocation the driver can size", name);
+    say(message, len, text);
+    return false;
+  }
+  if (at < base || at - base > size || size - (at - base) < bytes) {
+    std::snprintf(text, sizeof text,
+                  "tba_scene_cost_noalloc: %s length claims %zu bytes but its allocation holds %zu from that pointer",
+                  name, bytes, at >= base && at - base <= size ? size_t(size - (at - base)) : size_t(0));
+    say(message, len, text);
+    return false;
+  }
+  return true;
+}
+
 }  // namespace
 
-extern "C" tba_status tba_scene_cost_noalloc(const tba_control* control, const double* scene, const uint32_t* index,
-                                             double* result, void* stream, char* message, size_t message_len) {
+extern "C" tba_status tba_scene_cost_noalloc(const tba_control* control, const double* scene, size_t scene_len,
+                                             const uint32_t* index, size_t index_len, double* result,
+                                             size_t result_len, void* stream, char* message, size_t message_len) {
   say(message, message_len, "");
   if (!control || !scene || !index || !result) {
     say(message, message_len, "tba_scene_cost_noalloc: null control or device pointer");
@@ -139,12 +216,21 @@ extern "C" tba_status tba_scene_cost_noalloc(const tba_control* control, const d
     say(message, message_len, text);
     return TBA_ERROR_ARGUMENT;
   }
+  // The lengths the control implies: the packed arrays of tba_bundle_adjust, and 4 result words.
+  if (scene_len != tba_scene_size(control) || index_len != tba_index_size(control) || result_len < 4) {
+    char text[256];
+    std::snprintf(text, sizeof text,
+                  "tba_scene_cost_noalloc: array lengths (scene %zu, index %zu, result %zu) differ from the control's "
+                  "(scene %zu, index %zu, result 4)",
+                  scene_len, index_len, result_len, tba_scene_size(control), tba_index_size(control));
+    say(message, message_len, text);
+    return TBA_ERROR_ARGUMENT;
+  }
   if (reinterpret_cast<uintptr_t>(scene) % alignof(double) || reinterpret_cast<uintptr_t>(index) % alignof(uint32_t) ||
       reinterpret_cast<uintptr_t>(result) % alignof(double)) {
     say(message, message_len, "tba_scene_cost_noalloc: misaligned device pointer");
     return TBA_ERROR_ARGUMENT;
   }
-  // Set-up, once per device, with that device current: the scratch's device address.
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -154,16 +240,30 @@ extern "C" tba_status tba_scene_cost_noalloc(const tba_control* control, const d
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_setup);
-    if (!g_scratch[dev]) {
+    if (!driver_calls(message, message_len)) return TBA_ERROR_CUDA;
+    // Every buffer is checked before anything is launched.
+    if (!device_buffer(scene, scene_len * sizeof(double), dev, "scene", message, message_len) ||
+        !device_buffer(index, index_len * sizeof(uint32_t), dev, "index", message, message_len) ||
+        !device_buffer(result, 4 * sizeof(double), dev, "result", message, message_len))
+      return TBA_ERROR_ARGUMENT;
+    // Set-up, once per device and context, with that device current: the scratch's device address.
+    CUcontext ctx = nullptr;
+    if (g_context(&ctx) != CUDA_SUCCESS || !ctx) {
+      say(message, message_len, "tba_scene_cost_noalloc: no current CUDA context");
+      return TBA_ERROR_CUDA;
+    }
+    Scratch& slot = g_scratch[dev];
+    if (slot.context != ctx || !slot.address) {
       void* ptr = nullptr;
       e = cudaGetSymbolAddress(&ptr, g_tile_partials);
       if (e != cudaSuccess) {
         say(message, message_len, cudaGetErrorString(e));
         return TBA_ERROR_CUDA;
       }
-      g_scratch[dev] = static_cast<double*>(ptr);
+      slot.context = ctx;
+      slot.address = static_cast<double*>(ptr);
     }
-    scratch = g_scratch[dev];
+    scratch = slot.address;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   k_tile_cost<<<uint32_t(tiles), kThreads, 0, s>>>(scene, index, C, P, M, D, control->huber, scratch);

@@ -5,14 +5,16 @@
 //   k_obs_project   per observation: project the point in its camera; an inlier when the
 //                   projection is in the model's domain and its error is within the threshold
 //                   (projectIndexedObservations)
-//   k_obs_depth     per track (only with a depth bound): the linearised depth sensitivity of the
-//                   track's point to independent pixel noise, from its inlier observations with the
-//                   poses and intrinsics fixed; a track above the bound loses all its inliers
-//                   (filterIndexedObservationDepth, stableDepth).  One thread per track: groups of
-//                   8 lanes per track measured slower (fewer independent tracks in flight per warp);
-//                   capped at 64 registers for 8 blocks of 128 per SM (a few spilled words), which
-//                   hides more of its gathers' latency: 0.925 -> 0.873 ms over 1M tracks and
-//                   6.18M observations
+//   k_obs_tracks    with a depth bound: projectIndexedObservations fused with the depth filter
+//                   (filterIndexedObservationDepth, stableDepth): the linearised depth sensitivity
+//                   of each track's point to independent pixel noise, from its inlier
+//                   observations with the poses and intrinsics fixed; a track above the bound
+//                   loses all its inliers.  Observation-parallel: warp tasks of whole tracks (at
+//                   most 32 observations, one per lane; a longer track is a task of its own, swept
+//                   in rounds), the tracks' 3x3 information matrices summed by segmented warp
+//                   scans, every inlier's depth variance checked in its own lane, and a track's
+//                   verdict formed by a warp vote.  Each observation is read once and its flag and
+//                   error written once.
 //   k_obs_partials  the inlier error sum and count of each run of 64 observations, each run summed
 //                   in order (indexedObservationPartials), then k_obs_summary sums the runs in a
 //                   fixed tree (observationSummary)
@@ -26,9 +28,17 @@
 
 #include "tba_math.cuh"
 #include "tba_observations.cuh"
+#include "tba_warp.cuh"
 
 namespace tba {
 namespace {
+
+constexpr unsigned kObsFull = 0xffffffffu;
+
+__device__ inline void warp_sum7(double (&v)[7]) {
+  for (int d = 16; d > 0; d >>= 1)
+    for (int c = 0; c < 7; c++) v[c] += __shfl_xor_sync(kObsFull, v[c], d);
+}
 
 __device__ inline void obs_camera(const ObsParams& A, uint32_t i, double pose[12], Camera& k) {
   const double* r = A.cameras + 18 * size_t(A.indices[2 * size_t(i)]);
@@ -58,61 +68,165 @@ __global__ void __launch_bounds__(256) k_obs_project(ObsParams A) {
   }
 }
 
-// stableDepth: the information matrix of the point from the inlier observations (unweighted point
-// Jacobians), then for each inlier the variance of its camera-frame depth, sigma_z^2 = a^T A^-1 a
-// with a the camera's optical axis, against the relative bound noise * sigma_z / z.
-__device__ bool obs_stable_depth(const ObsParams& A, uint32_t start, uint32_t end, const double* X) {
-  double M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  uint32_t count = 0;
-  for (uint32_t i = start; i < end; i++) {
-    if (A.flags[i] == 0) continue;
-    count++;
-    double pose[12], q[3], pixel[2], du[3], dv[3];
-    Camera k;
-    obs_camera(A, i, pose, k);
-    obs_transform(pose, X, q);
-    if (!project(k, q, pixel, du, dv)) return false;
-    for (int row = 0; row < 2; row++) {
-      const double* g = row == 0 ? du : dv;
-      const double J[3] = {g[0] * pose[0] + g[1] * pose[3] + g[2] * pose[6],
-                           g[0] * pose[1] + g[1] * pose[4] + g[2] * pose[7],
-                           g[0] * pose[2] + g[1] * pose[5] + g[2] * pose[8]};
-      for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) M[3 * r + c] += J[r] * J[c];
-    }
-  }
-  if (count < 2) return false;
-  for (uint32_t i = start; i < end; i++) {
-    if (A.flags[i] == 0) continue;
-    double pose[12], q[3], s[3];
-    Camera k;
-    obs_camera(A, i, pose, k);
-    const double axis[3] = {pose[6], pose[7], pose[8]};
-    obs_transform(pose, X, q);
-    if (!solve3_spd(M, axis, s) || !(q[2] > 0)) return false;
-    const double variance = axis[0] * s[0] + axis[1] * s[1] + axis[2] * s[2];
-    if (!(variance >= 0)) return false;
-    const double relative = A.noise * sqrt(variance) / q[2];
-    if (!(relative <= A.max_relative_depth)) return false;
+// The point Jacobian rows' information (J^T J, 6 unique) of one observation of a track's point X,
+// and its camera-frame depth; false when the projection leaves the model's domain.
+__device__ inline bool obs_information(const double pose[12], const Camera& k, const double* X, double (&v)[6],
+                                       double& depth) {
+  double q[3], pixel[2], du[3], dv[3];
+  obs_transform(pose, X, q);
+  depth = q[2];
+  if (!project(k, q, pixel, du, dv)) return false;
+  for (int n = 0; n < 6; n++) v[n] = 0;
+  for (int row = 0; row < 2; row++) {
+    const double* g = row == 0 ? du : dv;
+    const double J[3] = {g[0] * pose[0] + g[1] * pose[3] + g[2] * pose[6], g[0] * pose[1] + g[1] * pose[4] + g[2] * pose[7],
+                         g[0] * pose[2] + g[1] * pose[5] + g[2] * pose[8]};
+    v[0] += J[0] * J[0];
+    v[1] += J[0] * J[1];
+    v[2] += J[0] * J[2];
+    v[3] += J[1] * J[1];
+    v[4] += J[1] * J[2];
+    v[5] += J[2] * J[2];
   }
   return true;
 }
 
-__global__ void __launch_bounds__(128, 8) k_obs_depth(ObsParams A) {
-  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= A.P) return;
-  const uint32_t start = A.offsets[h], end = A.offsets[h + 1];
-  A.flags[A.M + h] = 0;
-  if (end <= start) return;
-  uint32_t accepted = 0;
-  for (uint32_t i = start; i < end; i++) accepted += A.flags[i] != 0;
-  if (accepted < 2) return;
-  if (!obs_stable_depth(A, start, end, A.points + 3 * size_t(A.indices[2 * size_t(start) + 1]))) {
-    A.flags[A.M + h] = 1;
-    for (uint32_t i = start; i < end; i++) {
-      A.flags[i] = 0;
-      A.errors[i] = 0;
+// One inlier's share of stableDepth's verdict: its depth's relative standard deviation within the
+// bound, from the track's information v (6 unique) and the inlier's camera axis.
+__device__ inline bool obs_depth_ok(const ObsParams& A, const double (&v)[6], const double pose[12], double depth) {
+  const double M[9] = {v[0], v[1], v[2], v[1], v[3], v[4], v[2], v[4], v[5]};
+  const double axis[3] = {pose[6], pose[7], pose[8]};
+  double s[3];
+  if (!solve3_spd(M, axis, s) || !(depth > 0)) return false;
+  const double variance = axis[0] * s[0] + axis[1] * s[1] + axis[2] * s[2];
+  if (!(variance >= 0)) return false;
+  return A.noise * sqrt(variance) / depth <= A.max_relative_depth;
+}
+
+// One observation's projection against its pixel: inlier flag and error (projectIndexedObservations).
+__device__ inline bool obs_inlier(const ObsParams& A, uint32_t i, const double pose[12], const Camera& k, double& e) {
+  double q[3], pixel[2], du[3], dv[3];
+  obs_transform(pose, A.points + 3 * size_t(A.indices[2 * size_t(i) + 1]), q);
+  e = 0;
+  if (!project(k, q, pixel, du, dv)) return false;
+  const double x = pixel[0] - A.pixels[2 * size_t(i)], y = pixel[1] - A.pixels[2 * size_t(i) + 1];
+  e = sqrt(x * x + y * y);
+  return e <= A.max_error;
+}
+
+__global__ void __launch_bounds__(256) k_obs_tracks(ObsParams A) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < A.ntasks; t += warps) {
+    const uint32_t h0 = A.tasks[t], h1 = A.tasks[t + 1];
+    const uint32_t o0 = A.offsets[h0], n = A.offsets[h1] - o0;
+    if (n <= 32) {
+      // The task's tracks: a head bit at each non-empty track's first observation.
+      unsigned heads = 0;
+      for (uint32_t base = h0; base < h1; base += 32) {
+        const uint32_t h = base + uint32_t(lane);
+        unsigned bit = 0;
+        if (h < h1 && A.offsets[h + 1] > A.offsets[h]) bit = 1u << (A.offsets[h] - o0);
+        heads |= __reduce_or_sync(kObsFull, bit);
+      }
+      const bool valid = uint32_t(lane) < n;
+      const uint32_t i = o0 + (valid ? uint32_t(lane) : 0u);
+      const int head = valid ? 31 - __clz(heads & (kObsFull >> (31 - lane))) : lane;
+      double pose[12], e = 0;
+      Camera k;
+      obs_camera(A, i, pose, k);
+      const bool inlier = valid && obs_inlier(A, i, pose, k, e);
+      // The track's point is its first observation's.
+      const uint32_t xi = __shfl_sync(kObsFull, A.indices[2 * size_t(i) + 1], head);
+      double v[7] = {0, 0, 0, 0, 0, 0, 0}, depth = 0;
+      bool projected = true;
+      if (inlier) {
+        double w[6];
+        projected = obs_information(pose, k, A.points + 3 * size_t(xi), w, depth);
+        for (int c = 0; c < 6; c++) v[c] = projected ? w[c] : 0.0;
+        v[6] = 1;
+      }
+      const int seg = valid ? head : -1 - lane;
+      const Runs runs = lane_runs(seg, lane);
+      run_scan(v, runs);
+      const bool tail = valid && run_tail(runs, lane);
+      const unsigned tails = __ballot_sync(kObsFull, tail);
+      const int src = valid ? __ffs(tails & (kObsFull << lane)) - 1 : lane;
+      for (int c = 0; c < 7; c++) v[c] = __shfl_sync(kObsFull, v[c], src);
+      // Tracks with fewer than two inliers are not filtered.
+      const bool checked = v[6] >= 2;
+      bool ok = true;
+      if (inlier && checked) {
+        const double w[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+        ok = projected && obs_depth_ok(A, w, pose, depth);
+      }
+      const unsigned failed = __ballot_sync(kObsFull, inlier && checked && !ok);
+      // This lane's track: lanes head .. src.
+      const unsigned span = valid ? ((src == 31 ? kObsFull : ((1u << (src + 1)) - 1u)) & (kObsFull << head)) : 0u;
+      const bool rejected = (failed & span) != 0;
+      if (valid) {
+        const bool keep = inlier && !rejected;
+        A.flags[i] = keep ? 1u : 0u;
+        A.errors[i] = keep ? e : 0.0;
+      }
+      // Track flags: the head lane's verdict; empty tracks keep 0.
+      const unsigned verdicts = __ballot_sync(kObsFull, valid && uint32_t(lane) == uint32_t(head) && rejected);
+      for (uint32_t base = h0; base < h1; base += 32) {
+        const uint32_t h = base + uint32_t(lane);
+        if (h < h1) {
+          const uint32_t start = A.offsets[h];
+          A.flags[A.M + h] = (A.offsets[h + 1] > start && ((verdicts >> (start - o0)) & 1u)) ? 1u : 0u;
+        }
+      }
+      continue;
     }
+    // One track longer than 32 observations: rounds of 32 lanes.
+    const uint32_t xi = A.indices[2 * size_t(o0) + 1];
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    bool projected = true;
+    for (uint32_t base = 0; base < n; base += 32) {
+      const uint32_t i = o0 + base + uint32_t(lane);
+      if (i >= o0 + n) continue;
+      double pose[12], e, depth;
+      Camera k;
+      obs_camera(A, i, pose, k);
+      const bool inlier = obs_inlier(A, i, pose, k, e);
+      A.flags[i] = inlier ? 1u : 0u;
+      A.errors[i] = inlier ? e : 0.0;
+      if (inlier) {
+        double w[6];
+        if (obs_information(pose, k, A.points + 3 * size_t(xi), w, depth))
+          for (int c = 0; c < 6; c++) v[c] += w[c];
+        else
+          projected = false;
+        v[6] += 1;
+      }
+    }
+    warp_sum7(v);
+    const bool all_projected = __all_sync(kObsFull, projected);
+    bool ok = true;
+    if (v[6] >= 2) {
+      const double w[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+      for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t i = o0 + base + uint32_t(lane);
+        if (i >= o0 + n || A.flags[i] == 0) continue;
+        double pose[12], q[3];
+        Camera k;
+        obs_camera(A, i, pose, k);
+        obs_transform(pose, A.points + 3 * size_t(xi), q);
+        if (!obs_depth_ok(A, w, pose, q[2])) ok = false;
+      }
+      ok = __all_sync(kObsFull, ok) && all_projected;
+    }
+    if (lane == 0) A.flags[A.M + h0] = ok ? 0u : 1u;
+    if (!ok)
+      for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t i = o0 + base + uint32_t(lane);
+        if (i < o0 + n) {
+          A.flags[i] = 0;
+          A.errors[i] = 0;
+        }
+      }
   }
 }
 
@@ -159,8 +273,8 @@ __global__ void __launch_bounds__(1024) k_obs_summary(ObsParams A) {
 }  // namespace
 
 void launch_observations(const ObsParams& a, cudaStream_t s) {
-  if (a.M) k_obs_project<<<(a.M + 255) / 256, 256, 0, s>>>(a);
-  if (a.guarded && a.P) k_obs_depth<<<(a.P + 127) / 128, 128, 0, s>>>(a);
+  if (a.guarded && a.ntasks) k_obs_tracks<<<(a.ntasks + 7) / 8, 256, 0, s>>>(a);
+  else if (a.M) k_obs_project<<<(a.M + 255) / 256, 256, 0, s>>>(a);
   const uint32_t runs = (a.M + 63) / 64;
   if (runs) k_obs_partials<<<(runs + 255) / 256, 256, 0, s>>>(a);
   k_obs_summary<<<1, 1024, 0, s>>>(a);
@@ -188,7 +302,10 @@ void launch_observations(const ObsParams& a, cudaStream_t s) {
 // tile, and the producer writes the output tile back with one bulk store (cp.async.bulk
 // shared -> global).  Every DRAM byte moves once, in whole lines, with no register cost for the
 // bytes in flight (two blocks x two 34.8 KB tiles per SM).  Waits on an mbarrier are bounded: a
-// wait that runs out sets the error word and the block stops.
+// wait that runs out sets the error word to 1 and the block stops, after waiting (with the full
+// bound) for its own loads still in flight; a wait of that drain that runs out too sets it to 2.
+// The main-loop waits poll at most `wait_limit` times (kIdWaitLimit unless a test shortens it to
+// make them run out); the drain always uses kIdWaitLimit.
 namespace tba {
 namespace {
 
@@ -197,7 +314,7 @@ constexpr int kIdIn = 34, kIdOut = 23;
 constexpr int kIdStages = 2;
 constexpr uint32_t kIdTileIn = kIdRows * kIdIn * 8, kIdTileOut = kIdRows * kIdOut * 8;
 constexpr size_t kIdSmem = size_t(kIdStages) * kIdTileIn + kIdTileOut + 64;
-constexpr uint32_t kIdWaitLimit = 1u << 22;
+constexpr uint32_t kIdWaitLimit = kIdWaitPolls;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -215,8 +332,8 @@ __device__ __forceinline__ void id_load_tile(uint32_t bar, uint32_t dst, const v
                : "memory");
 }
 
-__device__ __forceinline__ bool id_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t k = 0; k < kIdWaitLimit; k++) {
+__device__ __forceinline__ bool id_wait(uint32_t bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t k = 0; k < limit; k++) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -282,7 +399,8 @@ __device__ __forceinline__ void inverse_depth_row(const double* m, double* o) {
 // An output tile (n * 184 bytes) is whole 16-byte words but for a last 8 bytes when n is odd; those
 // are written with a plain store.
 __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t count, const double* __restrict__ in,
-                                                                      double* __restrict__ out, uint32_t* error) {
+                                                                      double* __restrict__ out, uint32_t* error,
+                                                                      uint32_t wait_limit) {
   extern __shared__ __align__(128) unsigned char id_smem[];
   double* stage = reinterpret_cast<double*>(id_smem);
   double* tile_out = reinterpret_cast<double*>(id_smem + kIdStages * size_t(kIdTileIn));
@@ -307,8 +425,8 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
   for (; tile < tiles; tile += gridDim.x, k++) {
     const uint32_t s = k % kIdStages, parity = (k / kIdStages) & 1;
     const uint32_t n = rows_of(tile);
-    if (!id_wait(smem_addr(bars + s), parity)) {
-      atomicExch(error, 1u);
+    if (!id_wait(smem_addr(bars + s), parity, wait_limit)) {
+      atomicMax(error, 1u);
       abort_flag = 1;
     }
     // The previous tile's bulk store has to have read the output tile before it is rewritten.
@@ -336,24 +454,26 @@ __global__ void __launch_bounds__(kIdRows) k_linearize_inverse_depth(uint32_t co
   }
   // After a load that did not complete in time, let this block's loads still in flight (the
   // aborted tile's and those issued ahead of it) land before its shared memory is released; each
-  // wait is bounded.
+  // wait is bounded, and one that runs out is recorded as a drain failure (2).
   if (abort_flag && producer)
     for (uint32_t j = 0; j < uint32_t(kIdStages); j++)
-      if (tile + j * gridDim.x < tiles) id_wait(smem_addr(bars + (k + j) % kIdStages), ((k + j) / kIdStages) & 1);
+      if (tile + j * gridDim.x < tiles &&
+          !id_wait(smem_addr(bars + (k + j) % kIdStages), ((k + j) / kIdStages) & 1, kIdWaitLimit))
+        atomicMax(error, 2u);
   if (producer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 }  // namespace
 
 cudaError_t launch_linearize_inverse_depth(uint32_t count, const double* in, double* out, uint32_t* error,
-                                           int sms, cudaStream_t s) {
+                                           int sms, cudaStream_t s, uint32_t wait_limit) {
   if (!count) return cudaSuccess;
   const cudaError_t e =
       cudaFuncSetAttribute(k_linearize_inverse_depth, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kIdSmem));
   if (e != cudaSuccess) return e;
   const uint32_t tiles = (count + kIdRows - 1) / kIdRows;
   const uint32_t grid = std::min<uint32_t>(tiles, 2u * uint32_t(sms > 0 ? sms : 1));
-  k_linearize_inverse_depth<<<grid, kIdRows, kIdSmem, s>>>(count, in, out, error);
+  k_linearize_inverse_depth<<<grid, kIdRows, kIdSmem, s>>>(count, in, out, error, wait_limit);
   return cudaGetLastError();
 }
 

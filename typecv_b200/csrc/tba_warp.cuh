@@ -58,10 +58,10 @@ __device__ inline Runs lane_runs(int seg, int lane) {
 }
 
 // Inclusive sum within each run, in as many doubling steps as the longest run needs.
-template <int N>
-__device__ inline void run_scan(double (&v)[N], const Runs& r) {
+template <typename T, int N>
+__device__ inline void run_scan(T (&v)[N], const Runs& r) {
   for (int d = 1; d <= r.maxpos; d <<= 1) {
-    double t[N];
+    T t[N];
 #pragma unroll
     for (int n = 0; n < N; n++) t[n] = __shfl_up_sync(kFull, v[n], d);
     if (r.pos >= d) {
