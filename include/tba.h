@@ -43,12 +43,14 @@ typedef enum {
 } tba_status;
 
 /* Arithmetic of the solve.  TBA_PRECISION_FP64 is the drop-in (IEEE binary64 throughout).
- * TBA_PRECISION_MIXED runs the PCG's Schur product over an FP32 copy of the Jacobian factors, in
- * FP32 with FP64 sums across blocks, inside an FP64 LM loop (cost, gain, right-hand side, the
- * camera/point block inverses and the back-substitution stay FP64; the FP64 factors are kept too,
- * 12 x 4 more bytes per observation of device memory).  Each PCG solution is refined by its FP64
- * residual; when that residual is above the tolerance the PCG restarts from it on the FP64
- * product, with an iteration budget of its own.  It has no reference counterpart. */
+ * TBA_PRECISION_MIXED runs the PCG's Schur product over an FP32 copy of the Jacobian factors (and of
+ * the point-block inverses), in FP32 with each product block's camera sums in FP32 and the sums
+ * across blocks in FP64, inside an FP64 LM loop (cost, gain, right-hand side, the camera/point
+ * block inverses and the back-substitution stay FP64; the FP64 factors are kept too, 12 x 4 more
+ * bytes per observation of device memory).  Each PCG solution is refined by its FP64 residual (one
+ * product over the FP64 factors); when that residual is above the tolerance the PCG restarts from
+ * it on the FP32 product, at most twice, and then finishes on the FP64 product, each restart with
+ * an iteration budget of its own.  It has no reference counterpart. */
 typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
 
 /* TBA_FLAG_TIME_PRODUCTS: bracket every Schur product with CUDA events and report their total

@@ -59,6 +59,7 @@ struct tba_scene {
   double* scene = nullptr;     // device, tba_scene_size doubles
   uint32_t* index = nullptr;   // device, tba_index_size words
   void* plan = nullptr;        // HostPlan
+  uint32_t* plan_dev = nullptr;  // device copy of the plan's arrays (HostPlan::sections order)
 };
 
 namespace {
@@ -334,69 +335,16 @@ cudaEvent_t event(tba_device* d, size_t k) {
   return d->events[k];
 }
 
-// Stable counting sort of the point ids `in` by key[id] (< buckets) into `out`, on host threads:
-// per-thread histograms of contiguous ranges, offsets bucket-major then thread, ranges scattered in
-// order.
-void bucket_pass(const uint32_t* in, uint32_t n, const uint32_t* key, uint32_t buckets, uint32_t* out) {
-  const unsigned threads = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
-  std::vector<uint32_t> hist(size_t(threads) * buckets, 0);
-  const uint64_t serial_below = 1u << 16;
-  parallel_ranges(n, serial_below, [&](uint64_t b, uint64_t e, unsigned t) {
-    uint32_t* h = hist.data() + size_t(t) * buckets;
-    for (uint64_t i = b; i < e; i++) h[key[in[i]]]++;
-  });
-  uint32_t run = 0;
-  for (uint32_t b = 0; b < buckets; b++)
-    for (unsigned t = 0; t < threads; t++) {
-      const uint32_t count = hist[size_t(t) * buckets + b];
-      hist[size_t(t) * buckets + b] = run;
-      run += count;
-    }
-  parallel_ranges(n, serial_below, [&](uint64_t b, uint64_t e, unsigned t) {
-    uint32_t* h = hist.data() + size_t(t) * buckets;
-    for (uint64_t i = b; i < e; i++) out[h[key[in[i]]]++] = in[i];
-  });
-}
-
-// The engine's point order (tba_engine.cuh): the finite points sorted by the smallest, then the
-// largest camera observing them, stably; the directional points last, in their order.  Empty
-// (the caller's order) when the point offsets are not well formed; the device checks then fail the
-// problem before any kernel reads a schedule.
-std::vector<uint32_t> order_points(const uint32_t* obs_camera, const uint32_t* ps, uint32_t C, uint32_t P, uint32_t D,
-                                   uint32_t M) {
-  if (P == 0 || D > P || ps[0] != 0 || ps[P] != M) return {};
-  for (uint32_t p = 0; p < P; p++)
-    if (ps[p] > ps[p + 1]) return {};
-  const uint32_t F = P - D;
-  std::vector<uint32_t> lo(F), hi(F);
-  parallel_ranges(F, 1u << 15, [&](uint64_t b, uint64_t e, unsigned) {
-    for (uint64_t p = b; p < e; p++) {
-      uint32_t a = C - 1, z = 0;
-      for (uint32_t k = ps[p]; k < ps[p + 1]; k++) {
-        const uint32_t c = std::min(obs_camera[k], C - 1);  // out-of-range ids fail the checks later
-        a = std::min(a, c);
-        z = std::max(z, c);
-      }
-      lo[p] = a;
-      hi[p] = z;
-    }
-  });
-  std::vector<uint32_t> ids(F), by_hi(F), order(P);
-  std::iota(ids.begin(), ids.end(), 0u);
-  bucket_pass(ids.data(), F, hi.data(), C, by_hi.data());
-  bucket_pass(by_hi.data(), F, lo.data(), C, order.data());
-  for (uint32_t p = F; p < P; p++) order[p] = p;
-  return order;
-}
-
-// The host-side schedules of one problem's index: the engine's point order with the first
-// observation of each position, warp tasks over that order (with their first observations),
+// The host-side schedules of one problem's index: warp tasks (with their first observations),
 // camera chunks and the number of fixed cameras.
 struct HostPlan {
-  std::vector<uint32_t> order, pstart;  // empty order: the caller's order (pstart then unused)
   std::vector<uint32_t> tasks, task_obs;
   Chunks chunks;
   uint32_t fixed = 0;
+  // The arrays a solve uploads, in the order of a resident scene's device copy.
+  std::vector<const std::vector<uint32_t>*> sections() const {
+    return {&tasks, &task_obs, &chunks.cam, &chunks.beg, &chunks.cam_first};
+  }
 };
 
 HostPlan make_plan(const tba_control* ctl, const uint32_t* index, int sms) {
@@ -405,17 +353,9 @@ HostPlan make_plan(const tba_control* ctl, const uint32_t* index, int sms) {
   const uint32_t* cs = ps + P + 1;
   const uint32_t* active = cs + C + 1 + M;
   HostPlan plan;
-  plan.order = order_points(index, ps, C, P, ctl->directional_points, M);
-  const uint32_t* starts = ps;
-  if (!plan.order.empty()) {
-    plan.pstart.resize(size_t(P) + 1);
-    plan.pstart[0] = 0;
-    for (uint32_t q = 0; q < P; q++) plan.pstart[q + 1] = plan.pstart[q] + (ps[plan.order[q] + 1] - ps[plan.order[q]]);
-    starts = plan.pstart.data();
-  }
-  plan.tasks = build_tasks(starts, P);
+  plan.tasks = build_tasks(ps, P);
   plan.task_obs.resize(plan.tasks.size());
-  for (size_t t = 0; t < plan.tasks.size(); t++) plan.task_obs[t] = starts[plan.tasks[t]];
+  for (size_t t = 0; t < plan.tasks.size(); t++) plan.task_obs[t] = ps[plan.tasks[t]];
   plan.chunks = build_chunks(cs, C, M, sms);
   for (uint32_t c = 0; c < C; c++) plan.fixed += active[c] == 0;
   return plan;
@@ -434,6 +374,9 @@ struct SolveIO {
   // (with these host-side results, in the serial order) before any solver kernel runs.
   const HostChecks* checks = nullptr;
   double* check_ms = nullptr;  // receives the device checks' host wall time
+  // With `plan`: a device copy of its arrays (HostPlan::sections, concatenated), copied on the
+  // device instead of uploaded.
+  const uint32_t* plan_dev = nullptr;
 };
 
 void solve(tba_device* d, const tba_control* ctl, const double* scene, const uint32_t* index,
@@ -473,7 +416,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const bool mixed = ctl->precision == TBA_PRECISION_MIXED;
   p.factored = m <= tba::product_max_unknowns();
   p.Mpad = (M + 31) / 32 * 32;
-  const size_t factor_bytes = p.factored && !mixed ? size_t(tba::kFactors) * p.Mpad * 8 : 0;
+  const size_t factor_bytes = p.factored ? size_t(tba::kFactors) * p.Mpad * 8 : 0;
   const size_t factor32_bytes = p.factored && mixed ? size_t(tba::kFactors) * p.Mpad * 4 : 0;
   p.F = nullptr;
   p.F32 = mixed && p.factored ? reinterpret_cast<float*>(1) : nullptr;  // set below; selects the occupancy query
@@ -484,9 +427,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
                o_cams = L.take<double>(6 * size_t(C)), o_pixels = L.take<double>(2 * size_t(M)),
                o_tposes = L.take<double>(12 * size_t(C)), o_tpoints = L.take<double>(3 * size_t(P)),
                o_index = L.take<uint32_t>(3 * size_t(M) + P + 2 * size_t(C) + 2),
-               o_order = L.take<uint32_t>(P), o_pstart = L.take<uint32_t>(size_t(P) + 1),
-               o_ocam = L.take<uint32_t>(M), o_opt = L.take<uint32_t>(M), o_opix = L.take<double>(2 * size_t(M)),
-               o_sched = L.take<uint32_t>(p.factored ? M : 0), o_pblk32 = L.take<float>(mixed && p.factored ? 6 * size_t(P) : 0),
+               o_pblk32 = L.take<float>(mixed && p.factored ? 6 * size_t(P) : 0),
                o_tasks = L.take<uint32_t>(max_tasks), o_tobs = L.take<uint32_t>(max_tasks),
                o_ccam = L.take<uint32_t>(max_chunks),
                o_cbeg = L.take<uint32_t>(max_chunks + 1), o_cfirst = L.take<uint32_t>(C + 1),
@@ -528,17 +469,12 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.tposes = D(o_tposes);
   p.tpoints = D(o_tpoints);
   uint32_t* dindex = U32(o_index);
-  // The caller's sections; the point-major ones are replaced by their copies in the engine's point
-  // order once the plan is known (below).
   p.obs_camera = dindex;
   p.obs_point = dindex + M;
   p.point_start = dindex + 2 * size_t(M);
   p.camera_start = p.point_start + P + 1;
   p.camera_obs = p.camera_start + C + 1;
   p.active = p.camera_obs + M;
-  p.obs_point0 = p.obs_point;
-  p.pixels0 = p.pixels;
-  p.sched = p.factored ? U32(o_sched) : nullptr;
   p.pblk32 = mixed && p.factored ? reinterpret_cast<float*>(a + o_pblk32) : nullptr;
   p.tasks = U32(o_tasks);
   p.task_obs = U32(o_tobs);
@@ -551,7 +487,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   p.pblk = D(o_pblk);
   p.y = D(o_y);
   p.chunk_prod = D(o_cprod);
-  p.F = p.factored && !mixed ? D(o_F) : nullptr;
+  p.F = p.factored ? D(o_F) : nullptr;
   p.F32 = p.factored && mixed ? reinterpret_cast<float*>(a + o_F32) : nullptr;
   p.pw = D(o_pw);
   p.xw = D(o_xw);
@@ -602,17 +538,21 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   const uint32_t ntasks = tasks.empty() ? 0 : uint32_t(tasks.size() - 1), nchunks = uint32_t(chunks.cam.size());
   if (plannable) {
     if (tasks.size() > max_tasks || nchunks > max_chunks) throw Fail{TBA_ERROR_INTERNAL, "GPU BA schedule exceeds its bound"};
-    up_host(U32(o_tasks), tasks.data(), sizeof(uint32_t) * tasks.size());
-    up_host(U32(o_tobs), plan.task_obs.data(), sizeof(uint32_t) * plan.task_obs.size());
-    up_host(U32(o_ccam), chunks.cam.data(), sizeof(uint32_t) * nchunks);
-    up_host(U32(o_cbeg), chunks.beg.data(), sizeof(uint32_t) * (nchunks + 1));
-    up_host(U32(o_cfirst), chunks.cam_first.data(), sizeof(uint32_t) * (C + 1));
-    if (!plan.order.empty()) {
-      up_host(U32(o_order), plan.order.data(), sizeof(uint32_t) * P);
-      up_host(U32(o_pstart), plan.pstart.data(), sizeof(uint32_t) * (size_t(P) + 1));
+    // The plan's arrays: from the host, or from a resident scene's device copy.
+    const size_t dst[5] = {o_tasks, o_tobs, o_ccam, o_cbeg, o_cfirst};
+    size_t at = 0;
+    const auto sections = plan.sections();
+    for (size_t k = 0; k < sections.size(); k++) {
+      const std::vector<uint32_t>& v = *sections[k];
+      if (!v.empty()) {
+        if (io.plan_dev)
+          CUDA_TRY(cudaMemcpyAsync(U32(dst[k]), io.plan_dev + at, sizeof(uint32_t) * v.size(), cudaMemcpyDeviceToDevice, s));
+        else
+          up_host(U32(dst[k]), v.data(), sizeof(uint32_t) * v.size());
+      }
+      at += v.size();
     }
   }
-  const bool reordered = plannable && !plan.order.empty();
   p.normalize_scale = plan.fixed == 1;
   p.ntasks = ntasks;
   p.nchunks = nchunks;
@@ -653,20 +593,6 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   }
 
   uint32_t launches = 0, lm_done = 0, refinements = 0;
-  // The point-major sections in the engine's point order (after the checks: every offset valid).
-  if (reordered) {
-    const uint32_t* ps0 = p.point_start;
-    const uint32_t* oc0 = p.obs_camera;
-    p.obs_camera = U32(o_ocam);
-    p.obs_point = U32(o_opt);
-    p.pixels = D(o_opix);
-    p.point_start = U32(o_pstart);
-    tba::launch_reorder(p, U32(o_order), ps0, oc0, p.pixels0, s);
-    launches += p.factored ? 2 : 1;
-  } else if (p.factored) {
-    // The caller's order (a problem without a plan never gets here): tasks still need camera order.
-    tba::launch_reorder(p, nullptr, nullptr, nullptr, nullptr, s);
-  }
   // Event pairs around the Schur products; after the solve, only the products that ran PCG steps
   // (the first `steps` of each LM iteration; later ones are guarded no-ops) count.
   std::vector<std::pair<size_t, size_t>> product_events;
@@ -678,11 +604,10 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   launches += 4;
   CUDA_TRY(cudaGetLastError());
   bool lm_active = read_word(d, p.state, tba::S_ACTIVE) != 0;
-  // The mixed form's FP64 tail: the two-pass product, recomputing the FP64 Jacobians (the mixed
-  // form keeps FP32 factors only).
+  // The mixed form's FP64 tail: the one-pass product over the FP64 factors (the two-pass recompute
+  // product when the engine keeps no factors).
   tba::Params tail = p;
   tail.F32 = nullptr;
-  tail.factored = 0;
   tail.tol_inner = 0;  // the tail stops at the solve's own tolerance
   double product_error_max = 0, product_error_norm = 0;
   for (uint32_t it = 0; it < ctl->iterations && lm_active; it++) {
@@ -1083,28 +1008,49 @@ void solve_batch(tba_device* d, const tba_batch_control* bc, const tba_batch_pro
       run_mixed = mixed && hit->second < tba::kBatchShapes;
     } else {
       const auto t0 = std::chrono::steady_clock::now();
-      float best = 0;
       cudaEvent_t ta = event(d, 4), tb = event(d, 5);
+      // One timed launch of the batch in one form and shape; -1 when the shape does not fit.
+      auto trial_ms = [&](int k, bool form_mixed, uint32_t iterations) -> float {
+        const int blocks = blocks_of(k, form_mixed);
+        if (blocks <= 0) return -1;
+        tba::BatchArgs trial = form_mixed || !mixed ? args : args64;
+        trial.iterations = iterations;
+        CUDA_TRY(cudaMemsetAsync(trial.queue, 0, sizeof(uint32_t), s));
+        CUDA_TRY(cudaEventRecord(ta, s));
+        CUDA_TRY(tba::launch_batch(k, shared, form_mixed, trial, blocks, smem, s));
+        CUDA_TRY(cudaEventRecord(tb, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ta, tb));
+        return ms;
+      };
+      // Each form's shape by one LM iteration per shape; for a mixed request the two forms' best
+      // shapes then run the whole solve once each (one LM iteration does not show the refinement's
+      // share), and the faster form is kept.
+      int best_shape[2] = {-1, -1};
       for (int form = 0; form < (mixed ? 2 : 1); form++) {
         const bool form_mixed = mixed && form == 0;
-        tba::BatchArgs trial = form_mixed || !mixed ? args : args64;
-        trial.iterations = std::min<uint32_t>(args.iterations, 1);
+        float best = 0;
         for (int k = 0; k < tba::kBatchShapes; k++) {
-          const int blocks = blocks_of(k, form_mixed);
-          if (blocks <= 0) continue;
-          CUDA_TRY(cudaMemsetAsync(trial.queue, 0, sizeof(uint32_t), s));
-          CUDA_TRY(cudaEventRecord(ta, s));
-          CUDA_TRY(tba::launch_batch(k, shared, form_mixed, trial, blocks, smem, s));
-          CUDA_TRY(cudaEventRecord(tb, s));
-          CUDA_TRY(cudaStreamSynchronize(s));
-          float ms = 0;
-          CUDA_TRY(cudaEventElapsedTime(&ms, ta, tb));
-          if (shape < 0 || ms < best) {
+          const float ms = trial_ms(k, form_mixed, std::min<uint32_t>(args.iterations, 1));
+          if (ms >= 0 && (best_shape[form] < 0 || ms < best)) {
             best = ms;
-            shape = k;
-            run_mixed = form_mixed;
+            best_shape[form] = k;
           }
         }
+      }
+      shape = best_shape[0];
+      run_mixed = mixed;
+      if (mixed && best_shape[0] >= 0 && best_shape[1] >= 0 && args.iterations > 1) {
+        const float ms_mixed = trial_ms(best_shape[0], true, args.iterations);
+        const float ms_fp64 = trial_ms(best_shape[1], false, args.iterations);
+        if (ms_fp64 < ms_mixed) {
+          shape = best_shape[1];
+          run_mixed = false;
+        }
+      } else if (shape < 0) {
+        shape = best_shape[1];
+        run_mixed = false;
       }
       if (shape < 0) throw Fail{TBA_ERROR_INTERNAL, "no launch shape of the batched solver fits the device"};
       d->tuned[key] = shape + (mixed && !run_mixed ? tba::kBatchShapes : 0);
@@ -1807,16 +1753,21 @@ tba_status tba_scene_create(tba_device* d, const tba_control* shape, const doubl
     r->device = d;
     r->shape = *shape;
     r->plan = new HostPlan(make_plan(shape, index, d->sms));
+    std::vector<uint32_t> flat;
+    for (const std::vector<uint32_t>* v : static_cast<HostPlan*>(r->plan)->sections()) flat.insert(flat.end(), v->begin(), v->end());
     CUDA_TRY(cudaMalloc(&r->scene, scene_len * sizeof(double)));
     CUDA_TRY(cudaMalloc(&r->index, index_len * sizeof(uint32_t)));
+    CUDA_TRY(cudaMalloc(&r->plan_dev, std::max<size_t>(1, flat.size()) * sizeof(uint32_t)));
     CUDA_TRY(cudaMemcpyAsync(r->scene, scene, scene_len * sizeof(double), cudaMemcpyHostToDevice, d->stream));
     CUDA_TRY(cudaMemcpyAsync(r->index, index, index_len * sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
+    CUDA_TRY(cudaMemcpyAsync(r->plan_dev, flat.data(), flat.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
     CUDA_TRY(cudaStreamSynchronize(d->stream));
   } catch (const Fail& f) {
     d->error = f.message;
     if (r) {
       if (r->scene) cudaFree(r->scene);
       if (r->index) cudaFree(r->index);
+      if (r->plan_dev) cudaFree(r->plan_dev);
       delete static_cast<HostPlan*>(r->plan);
       delete r;
     }
@@ -1834,6 +1785,7 @@ void tba_scene_destroy(tba_scene* r) {
     cudaStreamSynchronize(r->device->stream);
     if (r->scene) cudaFree(r->scene);
     if (r->index) cudaFree(r->index);
+    if (r->plan_dev) cudaFree(r->plan_dev);
   }
   delete static_cast<HostPlan*>(r->plan);
   delete r;
@@ -1858,6 +1810,7 @@ tba_status tba_scene_adjust(tba_device* d, tba_scene* r, const tba_control* cont
     SolveIO io;
     io.device_source = true;
     io.plan = static_cast<const HostPlan*>(r->plan);
+    io.plan_dev = r->plan_dev;
     io.writeback = r->scene;
     io.state = state;
     solve(d, control, r->scene, r->index, output, report, io);

@@ -19,15 +19,7 @@
 // observations, one observation per lane, reduced per point with warp-shuffle segmented scans;
 // a point with more than 32 observations is a task of its own, swept in rounds of 32.  Camera
 // reductions run over the camera-major observation list in chunks of a fixed schedule.
-//
-// Point order.  The point-major kernels walk the points in the engine's own order: sorted by the
-// smallest, then the largest camera that observes them (stable; directional points last), so that
-// the points of one warp task share cameras.  The observations are copied into that order once
-// per solve (obs_camera, obs_point, pixels, point_start below are the reordered arrays; points keep
-// their ids, so every per-point array and the output stay in the caller's numbering).  Within a
-// task the one-pass product gives the lanes the task's observations in camera order (sched), so
-// observations of one camera sit in adjacent lanes: their camera sums reduce with a segmented warp
-// scan and one shared-memory atomic per camera and task instead of one per observation.
+
 #pragma once
 
 #include <cstdint>
@@ -87,22 +79,16 @@ struct Params {
   const double* pixels;  // 2M
   double* tposes;   // 12C
   double* tpoints;  // 3P
-  // index sections (point-major sections in the engine's point order)
+  // index sections
   const uint32_t* obs_camera;
   const uint32_t* obs_point;
-  const uint32_t* point_start;  // by position in the engine's point order
-  const uint32_t* obs_point0;   // the caller's point-major obsPoint and pixels (read through camera_obs)
-  const double* pixels0;
+  const uint32_t* point_start;
   const uint32_t* camera_start;
   const uint32_t* camera_obs;
   const uint32_t* active;
   // schedules
   const uint32_t* tasks;     // ntasks + 1 first points
   const uint32_t* task_obs;  // ntasks + 1 first observations
-  // Per observation of a task of at most 32: the camera-order lane's camera (bits 0-15) and its
-  // observation's offset in the task (bits 16-20), and the camera-order lane of the observation at
-  // this offset (bits 21-25).
-  const uint32_t* sched;
   uint32_t ntasks;
   const uint32_t* chunk_cam;    // nchunks
   const uint32_t* chunk_beg;    // nchunks + 1 positions in camera_obs
@@ -148,11 +134,6 @@ struct Params {
 };
 
 // Launches (tba_kernels.cu), each on stream `s`; grids come from `p`.
-// The observations in the engine's point order (new position q holds the caller's point order[q],
-// whose observations start at ps0[order[q]] in the caller's arrays oc0/px0), then each task's
-// camera-order lanes (sched).
-void launch_reorder(const Params& p, const uint32_t* order, const uint32_t* ps0, const uint32_t* oc0,
-                    const double* px0, cudaStream_t s);
 void launch_initialize(const Params& p, cudaStream_t s);
 void launch_cost(const Params& p, cudaStream_t s);
 void launch_finish_metrics(const Params& p, cudaStream_t s);

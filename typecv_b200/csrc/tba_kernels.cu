@@ -119,52 +119,9 @@ __global__ void k_setup(Params P) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < P.C) P.rlim[k] = radial_limit(P.cams[6 * size_t(k) + 4], P.cams[6 * size_t(k) + 5]);
   if (k < P.M) {
-    const uint32_t i = P.camera_obs[k];  // an observation of the caller's point-major order
-    P.cm_point[k] = P.obs_point0[i];
-    reinterpret_cast<double2*>(P.cm_pixel)[k] = reinterpret_cast<const double2*>(P.pixels0)[i];
-  }
-}
-
-// The observations in the engine's point order: position q holds the caller's point order[q],
-// whose observations move from ps0[order[q]] in the caller's arrays to point_start[q].  Runs after
-// the structural checks, so every offset is in range.
-__global__ void k_reorder(Params P, const uint32_t* order, const uint32_t* ps0, const uint32_t* oc0,
-                          const double* px0) {
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= P.P) return;
-  const uint32_t p = order[q], from = ps0[p], n = ps0[p + 1] - from, to = P.point_start[q];
-  uint32_t* oc = const_cast<uint32_t*>(P.obs_camera);
-  uint32_t* op = const_cast<uint32_t*>(P.obs_point);
-  double2* px = reinterpret_cast<double2*>(const_cast<double*>(P.pixels));
-  const double2* src = reinterpret_cast<const double2*>(px0);
-  for (uint32_t k = 0; k < n; k++) {
-    oc[to + k] = oc0[from + k];
-    op[to + k] = p;
-    px[to + k] = src[from + k];
-  }
-}
-
-// The camera order of each task of at most 32 observations (the one-pass product's lanes): the
-// task's observations sorted by camera, ties in point-major order.  One warp per task.
-__global__ void __launch_bounds__(256) k_task_order(Params P) {
-  __shared__ uint32_t slot[8][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t* sched = const_cast<uint32_t*>(P.sched);
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + warp; t < P.ntasks; t += warps) {
-    const uint32_t o0 = P.task_obs[t], n = P.task_obs[t + 1] - o0;
-    if (n > uint32_t(kTaskObs)) continue;  // a long point: swept in rounds, no camera order
-    const bool valid = uint32_t(lane) < n;
-    const uint32_t cam = valid ? P.obs_camera[o0 + lane] : 0u;
-    const uint32_t key = valid ? (cam << 5) | uint32_t(lane) : 0x80000000u | uint32_t(lane);  // cam < 2^16
-    uint32_t rank = 0;
-    for (int k = 0; k < 32; k++) rank += __shfl_sync(kFull, key, k) < key;
-    slot[warp][rank] = uint32_t(lane);  // camera-order lane `rank` takes offset `lane`
-    __syncwarp();
-    const uint32_t j = slot[warp][lane];
-    const uint32_t cj = __shfl_sync(kFull, cam, j);
-    if (valid) sched[o0 + lane] = cj | (j << 16) | (rank << 21);
-    __syncwarp();
+    const uint32_t i = P.camera_obs[k];
+    P.cm_point[k] = P.obs_point[i];
+    reinterpret_cast<double2*>(P.cm_pixel)[k] = reinterpret_cast<const double2*>(P.pixels)[i];
   }
 }
 
@@ -237,7 +194,7 @@ __device__ inline void point_obs(const Params& P, uint32_t i, uint32_t pt, doubl
     f[10] = g.jf[0];
     f[11] = g.jf[1];
     const size_t stride = P.Mpad;
-    // FP64 factors in the FP64 form, FP32 factors in the mixed form.
+    // FP64 factors always; the mixed form's PCG reads an FP32 copy.
     if (P.F)
       for (int k = 0; k < kFactors; k++) P.F[k * stride + i] = f[k];
     if (P.F32)
@@ -305,7 +262,6 @@ __global__ void __launch_bounds__(kPointThreads, TBA_POINT_MIN_BLOCKS) k_point_p
   uint32_t tb, te;
   block_tasks(P, tb, te);
   for (uint32_t t = tb + warp; t < te; t += nwarps) {
-    // Positions p0 <= q < p1 of the engine's point order; a lane's point id comes from obs_point.
     const uint32_t p0 = P.tasks[t], p1 = P.tasks[t + 1];
     const uint32_t o0 = P.point_start[p0], n = P.point_start[p1] - o0;
     if (n <= uint32_t(kTaskObs)) {
@@ -720,9 +676,8 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
   // It runs while the PCG is active, or, with P.refine, on the mixed form's refinement of x.
   if (P.state[S_CG_ACTIVE] == 0 && !(P.refine && P.state[S_REFINE] != 0)) return;
   const uint32_t m = P.m, C = P.C;
-  // The camera sums (6C values of A: FP64 for FP64 factors; for FP32 factors FP64 when they fit
-  // beside the staged direction, so that a warp's FP32 run sums accumulate in FP64, else FP32),
-  // then the staged direction: three arrays of C pairs of T (pair k of each camera's 6).
+  // The camera sums (6C values of A: a block's share of each camera), then the staged direction:
+  // three arrays of C pairs of T (pair k of each camera's 6).
   A* acc = reinterpret_cast<A*>(product_smem);
   using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
   T2* pws = reinterpret_cast<T2*>(reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, sizeof(A)));
@@ -750,22 +705,17 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
       e_next = P.task_obs[t + nwarps + 1];
     }
     if (n <= uint32_t(kTaskObs)) {
-      // Two lane orders over the task's n observations (offsets 0..n-1, point-major):
-      //  * point order: lane l holds offset l (its point pq), for the point sums
-      //    y_p = V_p^-1 sum_i W_i^T p;
-      //  * camera order: lane l takes offset j (camera c), the task's observations sorted by camera,
-      //    for the factors, the direction and the camera sums, which then reduce over runs of
-      //    adjacent lanes with one shared-memory atomic per camera.
-      // sched gives each lane its camera-order offset and camera, and the camera-order lane (inv)
-      // of its point-order offset.  Lanes >= n idle in both orders (j = inv = lane).  Every load a
-      // lane needs is issued before any arithmetic.
+      // One observation per lane (point-major), reduced per point with a segmented warp scan; each
+      // observation's camera share -W_i y_p goes to the block's camera sums with its own atomic
+      // adds.  (Grouping a task's observations by camera to add one share per camera was measured
+      // slower: points ordered so that a task's observations share cameras make their atomics
+      // collide, and the grouping's shuffles cost what it saves.)  Every load a lane needs is
+      // issued before any arithmetic; only the last lane of each point loads its V_p^-1.
       const bool valid = uint32_t(lane) < n;
-      const uint32_t w = valid ? __ldg(P.sched + o0 + lane) : (uint32_t(lane) << 16) | (uint32_t(lane) << 21);
-      const uint32_t pq = valid ? __ldg(P.obs_point + o0 + lane) : 0u;
-      const uint32_t c = valid ? (w & 0xffffu) : 0u, j = (w >> 16) & 31u, inv = (w >> 21) & 31u;
+      const uint32_t i = o0 + (valid ? uint32_t(lane) : 0u);
+      const uint32_t c = __ldg(P.obs_camera + i), pq = __ldg(P.obs_point + i);
       Factors<T> f;
-      load_factors(FT, stride, o0 + (valid ? j : 0u), f);
-      // Point order: the last lane of each point loads its V_p^-1.
+      load_factors(FT, stride, i, f);
       const uint32_t pn = __shfl_down_sync(kFull, pq, 1);
       const bool ptail = valid && (uint32_t(lane) + 1 == n || pn != pq);
       T vb[6] = {0, 0, 0, 0, 0, 0};
@@ -783,47 +733,35 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
         for (int k = 0; k < 6; k++) xw[k] = T(d[k]);
       }
       // A fixed camera's direction is zero, so its observations add nothing on the point side; their
-      // camera sums land in the fixed camera's rows, which k_product_columns discards.
-      const bool dir = directional(P, __shfl_sync(kFull, pq, j));
+      // camera shares land in the fixed camera's rows, which k_product_columns discards.
+      const bool dir = directional(P, pq);
       T sc[3] = {0, 0, 0};
       if (valid) factor_wt_t(f, xw, T(pf), dir, SHARED, sc);
-      T sq[3];
-      for (int k = 0; k < 3; k++) sq[k] = __shfl_sync(kFull, sc[k], inv);
       const Runs pr = lane_runs(valid ? int(pq) : -1 - lane, lane);
-      run_scan(sq, pr);
-      T yq[3] = {0, 0, 0};
+      run_scan(sc, pr);
+      T y[3] = {0, 0, 0};
       if (ptail) {
-        yq[0] = vb[0] * sq[0] + vb[1] * sq[1] + vb[2] * sq[2];
-        yq[1] = vb[1] * sq[0] + vb[3] * sq[1] + vb[4] * sq[2];
-        yq[2] = vb[2] * sq[0] + vb[4] * sq[1] + vb[5] * sq[2];
+        y[0] = vb[0] * sc[0] + vb[1] * sc[1] + vb[2] * sc[2];
+        y[1] = vb[1] * sc[0] + vb[3] * sc[1] + vb[4] * sc[2];
+        y[2] = vb[2] * sc[0] + vb[4] * sc[1] + vb[5] * sc[2];
       }
       const unsigned tails = __ballot_sync(kFull, ptail);
-      const int srcq = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
-      // Camera order again: each lane takes y_p of its observation's point.
-      const int src = __shfl_sync(kFull, srcq, j);
-      T y[3];
-      for (int k = 0; k < 3; k++) y[k] = __shfl_sync(kFull, yq[k], src);
-      // -W_i y_p in world axes (rotation rows q~ x h, translation rows h), summed per camera run.
-      T v[6] = {0, 0, 0, 0, 0, 0};
-      if (valid) {
-        const T gu = f.w * (f.ju[0] * y[0] + f.ju[1] * y[1] + f.ju[2] * y[2]);
-        const T gv = f.w * (f.jv[0] * y[0] + f.jv[1] * y[1] + f.jv[2] * y[2]);
-        if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
-        const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
-        v[0] = -(f.q[1] * h2 - f.q[2] * h1);
-        v[1] = -(f.q[2] * h0 - f.q[0] * h2);
-        v[2] = -(f.q[0] * h1 - f.q[1] * h0);
-        if (!dir) {
-          v[3] = -h0;
-          v[4] = -h1;
-          v[5] = -h2;
-        }
-      }
-      const Runs cr = lane_runs(valid ? int(c) : -1 - lane, lane);
-      run_scan(v, cr);
-      if (valid && run_tail(cr, lane)) {
-        A* ac = acc + c;
-        for (int k = 0; k < 6; k++) atomicAdd(ac + k * C, A(v[k]));
+      const int src = valid ? __ffs(tails & (kFull << lane)) - 1 : lane;
+      for (int k = 0; k < 3; k++) y[k] = __shfl_sync(kFull, y[k], src);
+      if (!valid) continue;
+      // -W_i y_p in world axes (rotation rows q~ x h, translation rows h).
+      const T gu = f.w * (f.ju[0] * y[0] + f.ju[1] * y[1] + f.ju[2] * y[2]);
+      const T gv = f.w * (f.jv[0] * y[0] + f.jv[1] * y[1] + f.jv[2] * y[2]);
+      if (SHARED) ef += double(gu * f.jf[0] + gv * f.jf[1]);
+      const T h0 = gu * f.ju[0] + gv * f.jv[0], h1 = gu * f.ju[1] + gv * f.jv[1], h2 = gu * f.ju[2] + gv * f.jv[2];
+      A* ac = acc + c;
+      atomicAdd(ac, A(-(f.q[1] * h2 - f.q[2] * h1)));
+      atomicAdd(ac + C, A(-(f.q[2] * h0 - f.q[0] * h2)));
+      atomicAdd(ac + 2 * C, A(-(f.q[0] * h1 - f.q[1] * h0)));
+      if (!dir) {
+        atomicAdd(ac + 3 * C, A(-h0));
+        atomicAdd(ac + 4 * C, A(-h1));
+        atomicAdd(ac + 5 * C, A(-h2));
       }
       continue;
     }
@@ -1156,9 +1094,9 @@ __global__ void __launch_bounds__(256) k_product_rows(Params P, int onepass, dou
 // ---- Mixed form: FP64 iterative refinement of the PCG solution ----------------------------------
 //
 // After the PCG ran on the FP32-factor product, k_refine_begin marks the refinement, an FP64 product
-// evaluates S x (launched with p := x: the two-pass product, which recomputes the FP64 Jacobians
-// from the poses, points and pixels, since the mixed form stores FP32 factors only; one pass over
-// stored FP64 factors where an engine keeps them), and k_refine forms the true residual
+// evaluates S x (launched with p := x: one pass over the FP64 factors, which the mixed form keeps
+// beside the FP32 ones because that costs less than recomputing the FP64 Jacobians in the two-pass
+// product, or that two-pass product when the engine keeps no factors), and k_refine forms the true residual
 // r = b - S x, z = M^-1 r, p = z, rho and r.r.  Its last block adds the focal row and either accepts
 // x (r.r within the tolerance: the PCG stays finished) or restarts the PCG from x with this r.
 
@@ -1555,14 +1493,11 @@ uint32_t product_finish_blocks(const Params& p) {
 
 uint32_t product_max_unknowns() { return uint32_t(kStagedSmemLimit / sizeof(double)) - 64; }
 
-// Bytes of a camera sum: FP64, except with FP32 factors when FP64 sums and the staged FP32
-// direction do not fit one block together.
-size_t product_sum_word(const Params& p) {
-  if (!p.F32) return sizeof(double);
-  return product_sums_bytes(p.C, sizeof(double)) + 6 * size_t(p.C) * sizeof(float) <= size_t(kStagedSmemLimit)
-             ? sizeof(double)
-             : sizeof(float);
-}
+// Bytes of a block's camera sum: the factors' type.  With FP32 factors a block sums its share of
+// each camera in FP32 (about 28 terms a camera and block at 1,500 cameras / 6.18M observations) and
+// the blocks' shares are summed in FP64; FP64 block sums (8-byte shared atomics) measured 14% slower
+// per product (0.138 against 0.121 ms there).
+size_t product_sum_word(const Params& p) { return p.F32 ? sizeof(float) : sizeof(double); }
 
 // The direction is staged in shared memory when the camera sums and it fit one block.
 bool product_staged(const Params& p) {
@@ -1588,7 +1523,6 @@ const void* product_kernel_of(const Params& p) {
   if (!p.F32)
     return st ? reinterpret_cast<const void*>(k_product_f<SHARED, double, double, true>)
               : reinterpret_cast<const void*>(k_product_f<SHARED, double, double, false>);
-  if (product_sum_word(p) == sizeof(double)) return reinterpret_cast<const void*>(k_product_f<SHARED, float, double, true>);
   return st ? reinterpret_cast<const void*>(k_product_f<SHARED, float, float, true>)
             : reinterpret_cast<const void*>(k_product_f<SHARED, float, float, false>);
 }
@@ -1608,8 +1542,6 @@ cudaError_t configure_kernels() {
       reinterpret_cast<const void*>(k_product_f<true, float, float, false>),
       reinterpret_cast<const void*>(k_product_f<false, float, float, true>),
       reinterpret_cast<const void*>(k_product_f<true, float, float, true>),
-      reinterpret_cast<const void*>(k_product_f<false, float, double, true>),
-      reinterpret_cast<const void*>(k_product_f<true, float, double, true>),
   };
   for (const void* f : kernels) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -1628,11 +1560,6 @@ int product_blocks_per_sm(const Params& p) {
   return n > 0 ? n : 1;
 }
 
-void launch_reorder(const Params& p, const uint32_t* order, const uint32_t* ps0, const uint32_t* oc0,
-                    const double* px0, cudaStream_t s) {
-  if (p.P && order) k_reorder<<<(p.P + 255) / 256, 256, 0, s>>>(p, order, ps0, oc0, px0);
-  if (p.factored && p.ntasks) k_task_order<<<(p.ntasks + 7) / 8, 256, 0, s>>>(p);
-}
 void launch_initialize(const Params& p, cudaStream_t s) {
   k_initialize<<<1, 1, 0, s>>>(p);
   const uint32_t n = p.M > p.C ? p.M : p.C;

@@ -40,10 +40,18 @@ __device__ inline void warp_sum7(double (&v)[7]) {
     for (int c = 0; c < 7; c++) v[c] += __shfl_xor_sync(kObsFull, v[c], d);
 }
 
+// The 18-word camera record of observation i, as nine 16-byte loads (records start 144-byte
+// aligned in a 16-byte aligned array).
 __device__ inline void obs_camera(const ObsParams& A, uint32_t i, double pose[12], Camera& k) {
-  const double* r = A.cameras + 18 * size_t(A.indices[2 * size_t(i)]);
-  for (int j = 0; j < 12; j++) pose[j] = r[j];
-  k = Camera{r[12], r[13], r[14], r[15], r[16], r[17]};
+  const double2* r = reinterpret_cast<const double2*>(A.cameras + 18 * size_t(A.indices[2 * size_t(i)]));
+  double w[18];
+  for (int j = 0; j < 9; j++) {
+    const double2 d = __ldg(r + j);
+    w[2 * j] = d.x;
+    w[2 * j + 1] = d.y;
+  }
+  for (int j = 0; j < 12; j++) pose[j] = w[j];
+  k = Camera{w[12], w[13], w[14], w[15], w[16], w[17]};
 }
 
 __device__ inline void obs_transform(const double pose[12], const double* X, double q[3]) {
@@ -68,14 +76,8 @@ __global__ void __launch_bounds__(256) k_obs_project(ObsParams A) {
   }
 }
 
-// The point Jacobian rows' information (J^T J, 6 unique) of one observation of a track's point X,
-// and its camera-frame depth; false when the projection leaves the model's domain.
-__device__ inline bool obs_information(const double pose[12], const Camera& k, const double* X, double (&v)[6],
-                                       double& depth) {
-  double q[3], pixel[2], du[3], dv[3];
-  obs_transform(pose, X, q);
-  depth = q[2];
-  if (!project(k, q, pixel, du, dv)) return false;
+// The point Jacobian rows' information (J^T J, 6 unique) from the projection's derivative rows.
+__device__ inline void information_rows(const double pose[12], const double du[3], const double dv[3], double (&v)[6]) {
   for (int n = 0; n < 6; n++) v[n] = 0;
   for (int row = 0; row < 2; row++) {
     const double* g = row == 0 ? du : dv;
@@ -88,6 +90,17 @@ __device__ inline bool obs_information(const double pose[12], const Camera& k, c
     v[4] += J[1] * J[2];
     v[5] += J[2] * J[2];
   }
+}
+
+// The information and camera-frame depth of one observation of a track's point X; false when the
+// projection leaves the model's domain.
+__device__ inline bool obs_information(const double pose[12], const Camera& k, const double* X, double (&v)[6],
+                                       double& depth) {
+  double q[3], pixel[2], du[3], dv[3];
+  obs_transform(pose, X, q);
+  depth = q[2];
+  if (!project(k, q, pixel, du, dv)) return false;
+  information_rows(pose, du, dv, v);
   return true;
 }
 
@@ -114,7 +127,7 @@ __device__ inline bool obs_inlier(const ObsParams& A, uint32_t i, const double p
   return e <= A.max_error;
 }
 
-__global__ void __launch_bounds__(256) k_obs_tracks(ObsParams A) {
+__global__ void __launch_bounds__(256, 2) k_obs_tracks(ObsParams A) {
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < A.ntasks; t += warps) {
@@ -132,17 +145,27 @@ __global__ void __launch_bounds__(256) k_obs_tracks(ObsParams A) {
       const bool valid = uint32_t(lane) < n;
       const uint32_t i = o0 + (valid ? uint32_t(lane) : 0u);
       const int head = valid ? 31 - __clz(heads & (kObsFull >> (31 - lane))) : lane;
-      double pose[12], e = 0;
+      // One projection per observation: its inlier flag and error, and (for an inlier of the
+      // track's own point, the usual case) its information and depth.
+      double pose[12], q[3], pixel[2], du[3], dv[3], e = 0;
       Camera k;
       obs_camera(A, i, pose, k);
-      const bool inlier = valid && obs_inlier(A, i, pose, k, e);
+      const uint32_t pi = A.indices[2 * size_t(i) + 1];
+      obs_transform(pose, A.points + 3 * size_t(pi), q);
+      bool inlier = valid && project(k, q, pixel, du, dv);
+      if (inlier) {
+        const double x = pixel[0] - A.pixels[2 * size_t(i)], y = pixel[1] - A.pixels[2 * size_t(i) + 1];
+        e = sqrt(x * x + y * y);
+        inlier = e <= A.max_error;
+      }
       // The track's point is its first observation's.
-      const uint32_t xi = __shfl_sync(kObsFull, A.indices[2 * size_t(i) + 1], head);
-      double v[7] = {0, 0, 0, 0, 0, 0, 0}, depth = 0;
+      const uint32_t xi = __shfl_sync(kObsFull, pi, head);
+      double v[7] = {0, 0, 0, 0, 0, 0, 0}, depth = q[2];
       bool projected = true;
       if (inlier) {
         double w[6];
-        projected = obs_information(pose, k, A.points + 3 * size_t(xi), w, depth);
+        if (xi == pi) information_rows(pose, du, dv, w);
+        else projected = obs_information(pose, k, A.points + 3 * size_t(xi), w, depth);
         for (int c = 0; c < 6; c++) v[c] = projected ? w[c] : 0.0;
         v[6] = 1;
       }
