@@ -627,6 +627,54 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // pair k of camera c at k * C + c, read as one 16- or 8-byte word): the lanes of a warp touch random
 // cameras, and with camera-major records of 6 words the 8-byte accesses of a warp would fall on only
 // 8 of the 16 bank pairs (6c mod 16 is even); component-major they spread over all of them.
+// The PCG direction of every camera in world axes, staged in shared memory for the one-pass
+// product, read at random cameras by the lanes of a warp.  FP32: one array of C float4 (the
+// rotation part and the first translation value) and one of C float2 (the rest), two loads a
+// lane; FP64: three arrays of C double2, three loads.  Component-major arrays spread random
+// cameras over all bank groups (a camera-major 6-word record would put a warp's accesses on only
+// half of them).
+template <typename T>
+struct StagedDirection;
+
+template <>
+struct StagedDirection<float> {
+  float4* a;
+  float2* b;
+  __device__ StagedDirection(unsigned char* base, uint32_t C)
+      : a(reinterpret_cast<float4*>(base)), b(reinterpret_cast<float2*>(base + 16 * size_t(C))) {}
+  __device__ void store(uint32_t c, const double* v) const {
+    a[c] = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
+    b[c] = make_float2(float(v[4]), float(v[5]));
+  }
+  __device__ void load(uint32_t c, float (&x)[6]) const {
+    const float4 u = a[c];
+    const float2 w = b[c];
+    x[0] = u.x;
+    x[1] = u.y;
+    x[2] = u.z;
+    x[3] = u.w;
+    x[4] = w.x;
+    x[5] = w.y;
+  }
+};
+
+template <>
+struct StagedDirection<double> {
+  double2* a;
+  uint32_t C;
+  __device__ StagedDirection(unsigned char* base, uint32_t C) : a(reinterpret_cast<double2*>(base)), C(C) {}
+  __device__ void store(uint32_t c, const double* v) const {
+    for (int k = 0; k < 3; k++) a[k * C + c] = make_double2(v[2 * k], v[2 * k + 1]);
+  }
+  __device__ void load(uint32_t c, double (&x)[6]) const {
+    for (int k = 0; k < 3; k++) {
+      const double2 u = a[k * C + c];
+      x[2 * k] = u.x;
+      x[2 * k + 1] = u.y;
+    }
+  }
+};
+
 // V_p^-1 (6 unique values) in the product's arithmetic type: the FP32 copy when the FP32 product
 // has one, else the FP64 block.
 template <typename T>
@@ -676,18 +724,14 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
   // It runs while the PCG is active, or, with P.refine, on the mixed form's refinement of x.
   if (P.state[S_CG_ACTIVE] == 0 && !(P.refine && P.state[S_REFINE] != 0)) return;
   const uint32_t m = P.m, C = P.C;
-  // The camera sums (6C values of A: a block's share of each camera), then the staged direction:
-  // three arrays of C pairs of T (pair k of each camera's 6).
+  // The camera sums (6C values of A: a block's share of each camera), then the staged direction
+  // (StagedDirection: 6 values of T per camera).
   A* acc = reinterpret_cast<A*>(product_smem);
-  using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-  T2* pws = reinterpret_cast<T2*>(reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, sizeof(A)));
+  const StagedDirection<T> pws{reinterpret_cast<unsigned char*>(product_smem) + product_sums_bytes(C, sizeof(A)), C};
   for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) acc[j] = A(0);
   if (threadIdx.x == 0) focal_acc = 0;
   if (STAGED)
-    for (uint32_t j = threadIdx.x; j < 3 * C; j += blockDim.x) {
-      const uint32_t c = j / 3, k = j % 3;
-      pws[k * C + c] = T2{T(P.pw[6 * c + 2 * k]), T(P.pw[6 * c + 2 * k + 1])};
-    }
+    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) pws.store(c, P.pw + 6 * size_t(c));
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const T* FT = sizeof(T) == 4 ? reinterpret_cast<const T*>(P.F32) : reinterpret_cast<const T*>(P.F);
@@ -722,11 +766,7 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
       if (ptail) load_point_inverse(P, pq, vb);
       T xw[6];
       if (STAGED) {
-        for (int k = 0; k < 3; k++) {
-          const T2 d = pws[k * C + c];
-          xw[2 * k] = d.x;
-          xw[2 * k + 1] = d.y;
-        }
+        pws.load(c, xw);
       } else {
         double d[6];
         load6(P.pw + 6 * size_t(c), d);
@@ -777,13 +817,11 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
         Factors<T> f;
         load_factors(FT, stride, i, f);
         double xw[6], u[3];
-        if (STAGED)
-          for (int k = 0; k < 3; k++) {
-            const T2 v = pws[k * C + c];
-            xw[2 * k] = double(v.x);
-            xw[2 * k + 1] = double(v.y);
-          }
-        else
+        if (STAGED) {
+          T d[6];
+          pws.load(c, d);
+          for (int k = 0; k < 6; k++) xw[k] = double(d[k]);
+        } else
           load6(P.pw + 6 * size_t(c), xw);
         factor_wt(f, xw, pf, true, directional(P, p0), SHARED, u);
         s[0] += u[0];
