@@ -307,12 +307,14 @@ def run_reference(args, world, rank):
     scene = make_scene(cfg, args.scale)
     for _ in range(args.warmup):
         cpu_baseline_run(scene, 1)
-    times, ran = [], 0
+    times, ran, cg = [], 0, 0
     threads = 1
+    n = 12 * scene.C + 3 * scene.P
     for _ in range(args.steps):
-        dt, k, threads, _ = cpu_baseline_run(scene, 1)
+        dt, k, threads, out = cpu_baseline_run(scene, 1)
         times.append(dt)
         ran += k
+        cg += int(out[n + 16])
     total = sum(times)
     value = ran / total
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
@@ -322,7 +324,8 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"1 LM iteration of the full {cfg} scene per step (the reference "
                                        "operator's algorithm restated in C++, oracle/ba_oracle.cpp)"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "pcg_iterations_per_s": cg / total}
     print(json.dumps(line), flush=True)
 
 
@@ -423,7 +426,8 @@ def form_summary(world, scene, reports, walls, out):
     return {"value": lm_all / t_max, "e2e": lm_all / e2e_max, "t_max": t_max,
             "pcg_iterations_per_s": cg_all / t_max, "final_cost": float(out[base + 6]),
             "final_rmse_px": float(out[base + 25]), "lm_iterations": lm, "cg_iterations": cg,
-            "refinements": sum(r.get("refinements", 0) for r in reports)}
+            "refinements": sum(r.get("refinements", 0) for r in reports),
+            "fp64_iterations": sum(r.get("fp64_iterations", 0) for r in reports)}
 
 
 def roofline(scene, reports, precision):
@@ -476,7 +480,7 @@ def run_single(args, world, rank, local):
     if head == "mixed":
         base = 12 * scene.C + 3 * scene.P
         line["mixed"] = {"refinements": summ["refinements"], "cg_iterations": summ["cg_iterations"],
-                         "pcg_failures": int(out[base + 17])}
+                         "fp64_iterations": summ["fp64_iterations"], "pcg_failures": int(out[base + 17])}
     if len(forms) == 2:
         r64, _, _, clk64, s64, inst64 = results["fp64"]
         line["fp64"] = {"value": s64["value"], "e2e": s64["e2e"], "pcg_iterations_per_s": s64["pcg_iterations_per_s"],
@@ -495,9 +499,13 @@ def run_single(args, world, rank, local):
         line["resident"] = results.get("resident")
     if world == 1 and not args.no_cpu_baseline:
         dt, ran, threads, ref = cpu_baseline_run(scene, 1)
+        cg = int(ref[12 * scene.C + 3 * scene.P + 16])
         line["cpu_baseline"] = {"value": ran / dt, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"1 LM iteration of the full {args.config} scene, {dt:.1f} s (the "
-                                          "reference operator's algorithm restated in C++, oracle/ba_oracle.cpp)"}
+                                          "reference operator's algorithm restated in C++, oracle/ba_oracle.cpp)",
+                                # The first LM iteration's PCG steps against the solve's average: the
+                                # same comparison per PCG iteration.
+                                "pcg_iterations": cg, "pcg_iterations_per_s": cg / dt}
         line["parity"] = parity_against_oracle(local, scene, ref, 1)
     print(json.dumps(line), flush=True)
 

@@ -50,11 +50,15 @@ typedef enum {
  * bytes per observation of device memory).  Each PCG solution is refined by its FP64 residual (one
  * product over the FP64 factors); when that residual is above the tolerance the PCG restarts from
  * it on the FP32 product, at most twice, and then finishes on the FP64 product, each restart with
- * an iteration budget of its own.  It has no reference counterpart. */
+ * an iteration budget of its own.  Once an LM iteration needed that FP64 finish, the call's later
+ * iterations solve on the FP64 product alone (tba_report.fp64_iterations).  It has no reference
+ * counterpart. */
 typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
 
 /* TBA_FLAG_TIME_PRODUCTS: bracket every Schur product with CUDA events and report their total
- * device time in tba_report.product_ms (a few microseconds of host work per PCG iteration). */
+ * device time in tba_report.product_ms (a few microseconds of host work per PCG iteration).
+ * Without it each PCG run is one launch of a CUDA graph that repeats the PCG step on the device
+ * until the PCG stops; with it the host launches the steps in chunks, with the same results. */
 #define TBA_FLAG_TIME_PRODUCTS 1u
 /* TBA_FLAG_PRODUCT_ERROR: once, on the first PCG direction of the first LM iteration, evaluate S p
  * with the solve's own Schur product and with the FP64 two-pass product (Jacobians recomputed from
@@ -95,7 +99,7 @@ typedef struct {
   double product_ms;      /* device time of the Schur products alone (sampled by events) */
   uint64_t h2d_bytes;
   uint64_t d2h_bytes;
-  uint32_t kernel_launches;
+  uint32_t kernel_launches; /* kernels launched by the call, those inside CUDA graphs included */
   uint32_t lm_iterations;  /* LM iterations that ran */
   uint32_t cg_iterations;  /* PCG iterations that ran (state word 16) */
   uint32_t product_launches; /* Schur products timed in product_ms */
@@ -104,6 +108,8 @@ typedef struct {
                                  on-chip memory) */
   uint32_t product_blocks; /* blocks of the one-pass product (each writes one partial row) */
   uint32_t refinements;    /* mixed form: PCG restarts from the FP64 residual */
+  uint32_t fp64_iterations; /* mixed form: LM iterations solved on the FP64 product alone, after an
+                              earlier iteration of the call needed the FP64 tail */
   double check_ms;         /* host wall time of the structural checks of the arrays (before wall_ms) */
   double product_error_max;  /* TBA_FLAG_PRODUCT_ERROR: max |S p - (S p)_64| / max |(S p)_64|, else 0 */
   double product_error_norm; /* TBA_FLAG_PRODUCT_ERROR: ||S p - (S p)_64|| / ||(S p)_64||, else 0 */

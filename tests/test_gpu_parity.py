@@ -308,6 +308,42 @@ def test_mixed_precision_through_the_operator(device):
     assert abs(mixed["diagnostics"]["finalCost"] - fp64["diagnostics"]["finalCost"]) < 1e-7
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_device_pcg_loop_matches_the_host_chunked_loop(device, precision):
+    # Each PCG run is one launch of a CUDA graph whose while node repeats the PCG step until the PCG
+    # stops or its budget is spent; with product timing on, the host issues the same steps in
+    # guarded chunks instead.  Both run the same kernels in the same order; the products' camera sums
+    # are atomic adds, whose order varies from run to run, so the results agree to the rounding that
+    # a PCG stopped at its tolerance carries through the LM iterations.  A second solve with the same
+    # launch parameters launches the graph built by the first.
+    scene = S.helix_scene(cameras=40, points=4000)
+    s, i = scene.packed()
+    base = 12 * scene.C + 3 * scene.P
+    cost_rel, pose_abs = (1e-12, 1e-6) if precision == 0 else (MIXED_REL, 1e-5)
+    for shared in (True, False):
+        kw = dict(anchor=0, scale_view=1, iterations=6, shared_focal=shared, tolerance=1e-8, max_cg=200,
+                  precision=precision)
+        chunked, rc = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M,
+                                                              flags=_lib.TBA_FLAG_TIME_PRODUCTS, **kw), s, i)
+        graph, rg = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, **kw), s, i)
+        again, ra = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, **kw), s, i)
+        assert rc["product_launches"] > 0 and rg["product_launches"] == 0 and ra["product_launches"] == 0
+        for out, rep in ((graph, rg), (again, ra)):
+            assert abs(out[base + 6] - chunked[base + 6]) <= cost_rel * chunked[base + 6]
+            assert np.max(np.abs(out[:12 * scene.C] - chunked[:12 * scene.C])) < pose_abs
+            assert rep["lm_iterations"] == rc["lm_iterations"]
+            if precision == 0:  # the mixed form's restarts turn rounding into whole PCG runs
+                assert abs(rep["cg_iterations"] - rc["cg_iterations"]) <= rc["lm_iterations"]
+        if precision == 0:
+            # The budget: with 3 PCG steps a solve, the loop stops at its budget, not at convergence.
+            budget = dict(kw, max_cg=3)
+            _, rb = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, **budget), s, i)
+            _, rbc = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M,
+                                                             flags=_lib.TBA_FLAG_TIME_PRODUCTS, **budget), s, i)
+            assert rb["lm_iterations"] == rbc["lm_iterations"] > 0
+            assert 0 < rb["cg_iterations"] == rbc["cg_iterations"] <= 3 * rb["lm_iterations"]
+
+
 def test_beyond_the_shared_memory_limit_the_two_pass_engine_matches_the_oracle(device):
     # 5,000 cameras: 30,000+ camera unknowns do not fit one block's shared memory, so the engine
     # takes the two-pass recompute product (report engine 1) in both forms.

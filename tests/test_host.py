@@ -39,6 +39,30 @@ def test_sizes_follow_the_reference_layout(lib):
     assert lib.tba_output_size(ctypes.byref(c)) == 12 * 7 + 3 * 11 + 26
 
 
+@pytest.mark.parametrize("struct, cname", [
+    (_lib.Control, "tba_control"), (_lib.Report, "tba_report"), (_lib.BatchProblem, "tba_batch_problem"),
+    (_lib.BatchControl, "tba_batch_control"), (_lib.BatchReport, "tba_batch_report"),
+    (_lib.VjpControl, "tba_vjp_control"), (_lib.VjpReport, "tba_vjp_report"),
+    (_lib.ObservationControl, "tba_observation_control"), (_lib.ObservationReport, "tba_observation_report"),
+])
+def test_ctypes_structures_match_the_header_layout(struct, cname, tmp_path):
+    # The Python mirrors of the C ABI's structures: the size and every field's offset as the C
+    # compiler lays out include/tba.h.
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    fields = [f[0] for f in struct._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "tba.h"\nint main(void) {\n'
+                   + f'  printf("%zu\\n", sizeof({cname}));\n'
+                   + "".join(f'  printf("%zu\\n", offsetof({cname}, {f}));\n' for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(struct), (cname, got[0], ctypes.sizeof(struct))
+    assert got[1:] == [getattr(struct, f).offset for f in fields], cname
+
+
 def test_device_open_reports_errors_without_crashing(lib):
     h = ctypes.c_void_p()
     status = lib.tba_device_open(0, ctypes.byref(h))

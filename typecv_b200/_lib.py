@@ -48,7 +48,8 @@ class Report(ctypes.Structure):
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint32), ("lm_iterations", ctypes.c_uint32),
         ("cg_iterations", ctypes.c_uint32), ("product_launches", ctypes.c_uint32), ("engine", ctypes.c_uint32),
-        ("product_blocks", ctypes.c_uint32), ("refinements", ctypes.c_uint32), ("check_ms", ctypes.c_double),
+        ("product_blocks", ctypes.c_uint32), ("refinements", ctypes.c_uint32),
+        ("fp64_iterations", ctypes.c_uint32), ("check_ms", ctypes.c_double),
         ("product_error_max", ctypes.c_double), ("product_error_norm", ctypes.c_double),
     ]
 

@@ -29,6 +29,24 @@
 
 using tba::Params;
 
+// The device-side PCG loop of one product form: a graph of one while node whose body is a PCG
+// step (product, column sums and alpha, x/r/z update and beta, new direction) and k_pcg_loop_next,
+// which counts the step and ends the loop when the PCG stops or its budget is spent.  The graph
+// bakes the launch parameters; `key` holds them, and a solve with the same parameters (the same
+// scene shape in the same workspace) launches it again instead of building a new one.
+struct PcgLoop {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<char> key;
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    key.clear();
+  }
+};
+
 struct tba_device {
   int ordinal = 0;
   int sms = 0;
@@ -49,6 +67,8 @@ struct tba_device {
   cudaGraphExec_t batch_graph = nullptr;
   std::vector<char> batch_key;
   std::map<std::string, int> tuned;
+  // The grid engine's device-side PCG loops: the solve's own product and the mixed form's FP64 tail.
+  PcgLoop pcg_loops[2];
 };
 
 // A scene resident on the device between calls: the packed arrays of one problem and its host
@@ -326,6 +346,50 @@ double read_word(tba_device* d, const double* state, int word) {
   return d->pinned[word];
 }
 
+// Makes `loop` run PCG steps with the launch parameters `q`: kept when it was built for the same
+// parameters, built again otherwise.
+cudaError_t build_pcg_loop(PcgLoop& loop, tba::Params q, cudaStream_t s) {
+  const char* bytes = reinterpret_cast<const char*>(&q);
+  if (loop.exec && loop.key.size() == sizeof q && std::memcmp(loop.key.data(), bytes, sizeof q) == 0)
+    return cudaSuccess;
+  loop.release();
+  cudaError_t e = cudaGraphCreate(&loop.graph, 0);
+  if (e != cudaSuccess) return e;
+  // The condition starts at 1 at every launch: the body runs at least once (its kernels are no-ops
+  // when the PCG is already stopped), then k_pcg_loop_next decides.
+  cudaGraphConditionalHandle handle;
+  e = cudaGraphConditionalHandleCreate(&handle, loop.graph, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = handle;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, loop.graph, nullptr, 0, &np);
+  if (e != cudaSuccess) return e;
+  tba::Params body = q;
+  body.pcg_loop = handle;
+  e = cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  tba::launch_product(body, s);
+  tba::launch_product_finish(body, s);
+  tba::launch_pcg_loop_next(body, s);
+  const cudaError_t launched = cudaGetLastError();
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(s, &captured);
+  if (launched != cudaSuccess) return launched;
+  if (e != cudaSuccess) return e;
+  e = cudaGraphInstantiate(&loop.exec, loop.graph, 0);
+  if (e != cudaSuccess) {
+    loop.exec = nullptr;
+    return e;
+  }
+  loop.key.assign(bytes, bytes + sizeof q);
+  return cudaSuccess;
+}
+
 cudaEvent_t event(tba_device* d, size_t k) {
   while (d->events.size() <= k) {
     cudaEvent_t e;
@@ -592,12 +656,18 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     if (!plannable) throw Fail{TBA_ERROR_INTERNAL, "GPU BA checks passed a problem without a schedule"};
   }
 
-  uint32_t launches = 0, lm_done = 0, refinements = 0;
+  uint32_t launches = 0, lm_done = 0, refinements = 0, fp64_iterations = 0;
+  // Mixed form: once an LM iteration's PCG needed the FP64 tail, the rest of the solve solves on the
+  // FP64 product (the FP32 product does not reach the tolerance on such a system, and its restarts
+  // would only add PCG runs).
+  bool fp64_only = false;
   // Event pairs around the Schur products; after the solve, only the products that ran PCG steps
   // (the first `steps` of each LM iteration; later ones are guarded no-ops) count.
   std::vector<std::pair<size_t, size_t>> product_events;
   std::vector<std::pair<size_t, uint32_t>> product_spans;  // (first event pair, real steps) per LM iteration
   const bool time_products = (ctl->flags & TBA_FLAG_TIME_PRODUCTS) != 0;
+  // Kernels per step of the device-side PCG loop launched last, while its step count is unread.
+  uint32_t loop_kernels = 0;
   tba::launch_initialize(p, s);
   tba::launch_cost(p, s);
   tba::launch_finish_metrics(p, s);
@@ -644,11 +714,24 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
       product_error_max = bmax > 0 ? dmax / bmax : dmax;
       product_error_norm = b2 > 0 ? std::sqrt(d2 / b2) : std::sqrt(d2);
     }
-    // PCG in chunks of guarded iterations; the read after each chunk only ends the loop early.
+    // PCG runs.  Untimed, a run is one launch of the form's device-side PCG loop, which ends on the
+    // device; its step count is taken from the next state read (every run is followed by one in the
+    // same LM iteration).  Timed, the steps run in chunks of guarded iterations with events around
+    // each product; the read after each chunk only ends the loop early.
     uint32_t done = 0, steps_before = 0;
     // `q` selects the product: the engine's own (FP32 factors in the mixed form), or the FP64
     // product of the mixed form's tail.  Only the engine's own products are timed.
     auto run_pcg = [&](uint32_t budget, const tba::Params& q, bool timed) {
+      if (!time_products) {
+        if (budget <= done) return;
+        PcgLoop& loop = d->pcg_loops[&q == &p ? 0 : 1];
+        CUDA_TRY(build_pcg_loop(loop, q, s));
+        tba::launch_pcg_loop_begin(q, budget - done, s);
+        launches++;
+        CUDA_TRY(cudaGraphLaunch(loop.exec, s));
+        loop_kernels = (q.factored ? 4 : 5) + 1;
+        return;
+      }
       const size_t first_pair = product_events.size();
       uint32_t chunk = 8;
       while (done < budget) {
@@ -664,7 +747,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
             tba::launch_product(q, s);
           }
           tba::launch_product_finish(q, s);
-          launches += q.factored ? 5 : 6;
+          launches += q.factored ? 4 : 5;
         }
         CUDA_TRY(cudaGetLastError());
         done += k;
@@ -676,25 +759,37 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
       if (time_products && timed) product_spans.emplace_back(first_pair, steps - steps_before);
       steps_before = steps;
     };
-    run_pcg(ctl->max_cg, p, true);
+    // After a state read: the steps of the device-side PCG loop that ran before it.
+    auto account_loop = [&]() {
+      if (!loop_kernels) return;
+      const uint32_t iters = uint32_t(d->pinned[tba::S_LOOP_ITERS]);
+      done += iters;
+      launches += iters * loop_kernels;
+      loop_kernels = 0;
+    };
+    if (fp64_only) fp64_iterations++;
+    run_pcg(ctl->max_cg, fp64_only ? tail : p, !fp64_only);
     // Mixed form: FP64 iterative refinement.  The true (FP64) residual of the FP32-product solution
     // restarts the PCG from that solution when it is above the tolerance; a restarted run (with an
     // iteration budget of its own) uses the FP32 product again and is checked again.  Only a
     // solution still above the tolerance after kFp32Restarts such runs is finished on the FP64
     // product, which resolves what FP32 factors cannot on badly conditioned systems.
-    if (mixed) {
+    if (mixed && !fp64_only) {
       constexpr int kFp32Restarts = 2;
       for (int round = 0;; round++) {
         tba::launch_refine(p, s);
         launches += 4;
         CUDA_TRY(cudaGetLastError());
-        if (read_word(d, p.state, tba::S_CG_ACTIVE) == 0) break;
+        const bool active = read_word(d, p.state, tba::S_CG_ACTIVE) != 0;
+        account_loop();
+        if (!active) break;
         refinements++;
         if (round < kFp32Restarts) {
           run_pcg(done + ctl->max_cg, p, true);
           continue;
         }
         run_pcg(done + ctl->max_cg, tail, false);
+        fp64_only = true;
         break;
       }
     }
@@ -705,8 +800,9 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     launches += 4;
     CUDA_TRY(cudaGetLastError());
     lm_done++;
-    CUDA_TRY(cudaMemcpyAsync(d->pinned, p.state, 32 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(d->pinned, p.state, 40 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    account_loop();
     lm_active = d->pinned[tba::S_ACTIVE] != 0;
   }
   tba::launch_pack(p, s);
@@ -762,6 +858,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     report->engine = p.factored ? 0 : 1;
     report->product_blocks = p.factored ? p.prod_blocks : 0;
     report->refinements = uint32_t(refinements);
+    report->fp64_iterations = fp64_iterations;
     report->product_error_max = product_error_max;
     report->product_error_norm = product_error_norm;
     report->wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
@@ -1534,6 +1631,7 @@ void tba_device_close(tba_device* d) {
   if (d->down) cudaStreamSynchronize(d->down);
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
   if (d->batch_graph) cudaGraphExecDestroy(d->batch_graph);
+  for (PcgLoop& loop : d->pcg_loops) loop.release();
   if (d->batch_arena) cudaFree(d->batch_arena);
   if (d->arena) cudaFree(d->arena);
   if (d->pinned) cudaFreeHost(d->pinned);

@@ -22,6 +22,8 @@
 
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "tba_math.cuh"
@@ -50,6 +52,8 @@ enum StateWord : int {
   S_REFINE = 34,           // an FP64 refinement of the PCG solution is under way
   S_REFINED = 35,          // refinements that restarted the PCG (this solve)
   S_INNER_R0 = 36,         // residual^2 that the current inner PCG run is measured against
+  S_LOOP_ITERS = 37,       // PCG-step launches of the current device-side PCG loop
+  S_LOOP_LIMIT = 38,       // the launches that loop may make (its iteration budget)
   S_WORDS = 64
 };
 
@@ -131,6 +135,9 @@ struct Params {
   uint32_t* ticket;   // last-block counters
   double* state;      // S_WORDS
   double* output;
+  // The condition of the CUDA graph's while node that runs the PCG steps on the device (set by
+  // k_pcg_loop_next inside the loop's body graph; unused outside it).
+  cudaGraphConditionalHandle pcg_loop;
 };
 
 // Launches (tba_kernels.cu), each on stream `s`; grids come from `p`.
@@ -145,6 +152,11 @@ void launch_product(const Params& p, cudaStream_t s);
 // One PCG step after the product: column reduction of the product partials and alpha, the
 // distributed update of x, r, z and beta, then the new direction p.
 void launch_product_finish(const Params& p, cudaStream_t s);
+// The device-side PCG loop (a CUDA graph with a while node whose body is one PCG step): its
+// iteration budget, set on the stream before the graph's launch, and the body's last kernel, which
+// counts the step and keeps the loop going while the PCG is active and within the budget.
+void launch_pcg_loop_begin(const Params& p, uint32_t limit, cudaStream_t s);
+void launch_pcg_loop_next(const Params& p, cudaStream_t s);
 // Mixed form: the FP64 residual r = b - S x of the PCG solution (the two-pass recompute product
 // on x), and the PCG restarted from it when it is above the tolerance.
 void launch_refine(const Params& p, cudaStream_t s);

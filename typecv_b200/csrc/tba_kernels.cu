@@ -1129,6 +1129,26 @@ __global__ void __launch_bounds__(256) k_product_rows(Params P, int onepass, dou
   }
 }
 
+// ---- The device-side PCG loop --------------------------------------------------------------------
+//
+// A solve runs its PCG steps as one CUDA graph: a while node whose body is one step (the product,
+// the column sums with alpha, the x/r/z update with beta, the new direction) followed by
+// k_pcg_loop_next.  The loop ends on the device when the PCG stops (converged, broken down) or its
+// budget of steps is spent, with no host round trip per step and no launches past convergence.
+// k_pcg_loop_next runs at the end of every body iteration, so the loop always ends within its budget.
+
+__global__ void k_pcg_loop_begin(Params P, uint32_t limit) {
+  P.state[S_LOOP_ITERS] = 0;
+  P.state[S_LOOP_LIMIT] = limit;
+}
+
+__global__ void k_pcg_loop_next(Params P) {
+  double* st = P.state;
+  const double iters = st[S_LOOP_ITERS] + 1;
+  st[S_LOOP_ITERS] = iters;
+  cudaGraphSetConditional(P.pcg_loop, st[S_CG_ACTIVE] != 0 && iters < st[S_LOOP_LIMIT] ? 1u : 0u);
+}
+
 // ---- Mixed form: FP64 iterative refinement of the PCG solution ----------------------------------
 //
 // After the PCG ran on the FP32-factor product, k_refine_begin marks the refinement, an FP64 product
@@ -1639,6 +1659,8 @@ void launch_product_finish(const Params& p, cudaStream_t s) {
   k_pcg_update<<<(p.m + kUpdateRows - 1) / kUpdateRows, kUpdateThreads, 0, s>>>(p);
   k_pcg_direction<<<(p.C + 1 + 255) / 256, 256, 0, s>>>(p);
 }
+void launch_pcg_loop_begin(const Params& p, uint32_t limit, cudaStream_t s) { k_pcg_loop_begin<<<1, 1, 0, s>>>(p, limit); }
+void launch_pcg_loop_next(const Params& p, cudaStream_t s) { k_pcg_loop_next<<<1, 1, 0, s>>>(p); }
 void launch_refine(const Params& p, cudaStream_t s) {
   k_refine_begin<<<1, 1, 0, s>>>(p);
   Params q = p;
