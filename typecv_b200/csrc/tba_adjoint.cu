@@ -620,6 +620,20 @@ __global__ void __launch_bounds__(1024) k_adj_vec(AdjParams A) {
   }
 }
 
+// The device-side PCG loop: k_adj_loop_next runs at the end of every body iteration, so the loop
+// ends within its budget; it ends earlier when the PCG stops.
+__global__ void k_adj_loop_begin(AdjParams A, uint32_t limit) {
+  A.state[A_LOOP_ITERS] = 0;
+  A.state[A_LOOP_LIMIT] = limit;
+}
+
+__global__ void k_adj_loop_next(AdjParams A) {
+  double* st = A.state;
+  const double iters = st[A_LOOP_ITERS] + 1;
+  st[A_LOOP_ITERS] = iters;
+  cudaGraphSetConditional(A.loop, st[A_ACTIVE] != 0 && iters < st[A_LOOP_LIMIT] ? 1u : 0u);
+}
+
 __global__ void __launch_bounds__(256) k_adj_back(AdjParams A) {
   for (uint32_t pt = blockIdx.x * blockDim.x + threadIdx.x; pt < A.P; pt += gridDim.x * blockDim.x) {
     double t[3] = {A.bp[3 * size_t(pt)], A.bp[3 * size_t(pt) + 1], A.bp[3 * size_t(pt) + 2]};
@@ -912,6 +926,16 @@ uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s, cudaEvent_t bef
   }
   k_adj_vec<<<1, 1024, 0, s>>>(a);
   return 3;
+}
+
+uint32_t adj_launch_loop_begin(const AdjParams& a, uint32_t limit, cudaStream_t s) {
+  k_adj_loop_begin<<<1, 1, 0, s>>>(a, limit);
+  return 1;
+}
+
+uint32_t adj_launch_loop_next(const AdjParams& a, cudaStream_t s) {
+  k_adj_loop_next<<<1, 1, 0, s>>>(a);
+  return 1;
 }
 
 uint32_t adj_launch_back_substitute(const AdjParams& a, cudaStream_t s) {

@@ -32,7 +32,10 @@ namespace tba {
 enum AdjWord : int {
   A_RHO = 0, A_ALPHA = 1, A_BETA = 2, A_R0 = 3, A_R2 = 4, A_ACTIVE = 5, A_FAILED = 6, A_STEPS = 7,
   A_POINT_FAILED = 8, A_CAMERA_FAILED = 9, A_GNORM = 10, A_SBAR = 11, A_KBAR = 12, A_DOT = 13,
-  A_BASELINE = 14, A_ORIGIN = 15, A_SCALE = 18, A_INVALID = 19, A_COST = 20, A_POINT_SINGULAR = 21, A_WORDS = 32
+  A_BASELINE = 14, A_ORIGIN = 15, A_SCALE = 18, A_INVALID = 19, A_COST = 20, A_POINT_SINGULAR = 21,
+  A_LOOP_ITERS = 22,  // PCG steps of the current device-side PCG loop
+  A_LOOP_LIMIT = 23,  // the steps that loop may take
+  A_WORDS = 32
 };
 
 struct AdjParams {
@@ -85,6 +88,10 @@ struct AdjParams {
   uint32_t prod_blocks;      // 0: the two-pass product
   uint32_t prod_copies;      // copies of the camera sums in a block's shared memory (warp w adds to w % copies)
   double* part;              // prod_blocks x 6C
+  // The condition of the CUDA graph's while node that runs the PCG steps on the device (set by
+  // k_adj_loop_next inside the loop's body graph; unused outside it).  The step kernels read
+  // neither `mu` nor `rhs_mode`.
+  cudaGraphConditionalHandle loop;
 };
 
 // The largest camera count of the one-pass product (its camera sums in one block's shared memory).
@@ -101,6 +108,11 @@ uint32_t adj_launch_pcg_init(const AdjParams& a, cudaStream_t s);
 // Product + vector step; with events, the one-pass product's launch is bracketed by them.
 uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s, cudaEvent_t before = nullptr,
                              cudaEvent_t after = nullptr);
+// The device-side PCG loop (a CUDA graph with a while node whose body is one PCG step): its step
+// budget, set on the stream before the graph's launch, and the body's last kernel, which counts the
+// step and keeps the loop going while the PCG is active and within the budget.
+uint32_t adj_launch_loop_begin(const AdjParams& a, uint32_t limit, cudaStream_t s);
+uint32_t adj_launch_loop_next(const AdjParams& a, cudaStream_t s);
 uint32_t adj_launch_back_substitute(const AdjParams& a, cudaStream_t s);
 // The candidate theta (+) delta into tposes/tpoints (with the gauge normalisation) and its robust
 // cost into A_COST; then, when accepted, its commit.

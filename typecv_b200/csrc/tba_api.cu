@@ -38,6 +38,7 @@ struct PcgLoop {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::vector<char> key;
+  uint32_t body_kernels = 0;  // kernels of one body iteration
   void release() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -67,8 +68,10 @@ struct tba_device {
   cudaGraphExec_t batch_graph = nullptr;
   std::vector<char> batch_key;
   std::map<std::string, int> tuned;
-  // The grid engine's device-side PCG loops: the solve's own product and the mixed form's FP64 tail.
+  // The grid engine's device-side PCG loops (the solve's own product and the mixed form's FP64
+  // tail) and the adjoint's.
   PcgLoop pcg_loops[2];
+  PcgLoop adj_loop;
 };
 
 // A scene resident on the device between calls: the packed arrays of one problem and its host
@@ -346,17 +349,19 @@ double read_word(tba_device* d, const double* state, int word) {
   return d->pinned[word];
 }
 
-// Makes `loop` run PCG steps with the launch parameters `q`: kept when it was built for the same
-// parameters, built again otherwise.
-cudaError_t build_pcg_loop(PcgLoop& loop, tba::Params q, cudaStream_t s) {
-  const char* bytes = reinterpret_cast<const char*>(&q);
-  if (loop.exec && loop.key.size() == sizeof q && std::memcmp(loop.key.data(), bytes, sizeof q) == 0)
+// Makes `loop` a graph of one while node whose body `capture(handle, stream)` records (returning its
+// kernel count): kept when it was built for the same `key` (the launch parameters its kernels bake),
+// built again otherwise.
+template <class Capture>
+cudaError_t build_device_loop(PcgLoop& loop, const void* key, size_t key_len, cudaStream_t s, Capture capture) {
+  const char* bytes = static_cast<const char*>(key);
+  if (loop.exec && loop.key.size() == key_len && std::memcmp(loop.key.data(), bytes, key_len) == 0)
     return cudaSuccess;
   loop.release();
   cudaError_t e = cudaGraphCreate(&loop.graph, 0);
   if (e != cudaSuccess) return e;
   // The condition starts at 1 at every launch: the body runs at least once (its kernels are no-ops
-  // when the PCG is already stopped), then k_pcg_loop_next decides.
+  // when the PCG is already stopped), then the body's last kernel decides.
   cudaGraphConditionalHandle handle;
   e = cudaGraphConditionalHandleCreate(&handle, loop.graph, 1, cudaGraphCondAssignDefault);
   if (e != cudaSuccess) return e;
@@ -368,14 +373,10 @@ cudaError_t build_pcg_loop(PcgLoop& loop, tba::Params q, cudaStream_t s) {
   cudaGraphNode_t node;
   e = cudaGraphAddNode(&node, loop.graph, nullptr, 0, &np);
   if (e != cudaSuccess) return e;
-  tba::Params body = q;
-  body.pcg_loop = handle;
   e = cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                     cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
-  tba::launch_product(body, s);
-  tba::launch_product_finish(body, s);
-  tba::launch_pcg_loop_next(body, s);
+  loop.body_kernels = capture(handle, s);
   const cudaError_t launched = cudaGetLastError();
   cudaGraph_t captured = nullptr;
   e = cudaStreamEndCapture(s, &captured);
@@ -386,8 +387,35 @@ cudaError_t build_pcg_loop(PcgLoop& loop, tba::Params q, cudaStream_t s) {
     loop.exec = nullptr;
     return e;
   }
-  loop.key.assign(bytes, bytes + sizeof q);
+  loop.key.assign(bytes, bytes + key_len);
   return cudaSuccess;
+}
+
+// The grid engine's PCG loop for the launch parameters `q`.
+cudaError_t build_pcg_loop(PcgLoop& loop, const tba::Params& q, cudaStream_t s) {
+  return build_device_loop(loop, &q, sizeof q, s, [&](cudaGraphConditionalHandle handle, cudaStream_t cs) {
+    tba::Params body = q;
+    body.pcg_loop = handle;
+    tba::launch_product(body, cs);
+    tba::launch_product_finish(body, cs);
+    tba::launch_pcg_loop_next(body, cs);
+    return uint32_t(q.factored ? 4 : 5) + 1;
+  });
+}
+
+// The adjoint's PCG loop: the step kernels read neither the damping nor the right-hand side's mode,
+// so one graph serves every linear solve of a vjp (and of the next call with the same arrays).
+cudaError_t build_adjoint_loop(PcgLoop& loop, const tba::AdjParams& a, cudaStream_t s) {
+  tba::AdjParams key = a;
+  key.mu = 0;
+  key.rhs_mode = 0;
+  key.loop = 0;
+  return build_device_loop(loop, &key, sizeof key, s, [&](cudaGraphConditionalHandle handle, cudaStream_t cs) {
+    tba::AdjParams body = key;
+    body.loop = handle;
+    const uint32_t step = tba::adj_launch_pcg_step(body, cs);
+    return step + tba::adj_launch_loop_next(body, cs);
+  });
 }
 
 cudaEvent_t event(tba_device* d, size_t k) {
@@ -729,7 +757,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
         tba::launch_pcg_loop_begin(q, budget - done, s);
         launches++;
         CUDA_TRY(cudaGraphLaunch(loop.exec, s));
-        loop_kernels = (q.factored ? 4 : 5) + 1;
+        loop_kernels = loop.body_kernels;
         return;
       }
       const size_t first_pair = product_events.size();
@@ -1367,6 +1395,14 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     CUDA_TRY(cudaGetLastError());
     uint32_t done = 0;
     const bool timed = time_products && A.prod_blocks;
+    const bool on_device = !timed && vc->max_cg > 0;
+    if (on_device) {
+      // One launch of the device-side PCG loop, which stops on the device.
+      CUDA_TRY(build_adjoint_loop(d->adj_loop, A, s));
+      launches += tba::adj_launch_loop_begin(A, vc->max_cg, s);
+      CUDA_TRY(cudaGraphLaunch(d->adj_loop.exec, s));
+      done = vc->max_cg;
+    }
     while (done < vc->max_cg) {
       const uint32_t k = std::min<uint32_t>(16, vc->max_cg - done);
       for (uint32_t j = 0; j < k; j++)
@@ -1388,6 +1424,7 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
       if (d->pinned[tba::A_ACTIVE] == 0) break;
     }
     read_state();
+    if (on_device) launches += uint32_t(d->pinned[tba::A_LOOP_ITERS]) * d->adj_loop.body_kernels;
     const double* st = d->pinned;
     cg_total += uint32_t(st[tba::A_STEPS]);
     last_residual = st[tba::A_R0] > 0 ? std::sqrt(st[tba::A_R2] / st[tba::A_R0]) : 0;
@@ -1632,6 +1669,7 @@ void tba_device_close(tba_device* d) {
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
   if (d->batch_graph) cudaGraphExecDestroy(d->batch_graph);
   for (PcgLoop& loop : d->pcg_loops) loop.release();
+  d->adj_loop.release();
   if (d->batch_arena) cudaFree(d->batch_arena);
   if (d->arena) cudaFree(d->arena);
   if (d->pinned) cudaFreeHost(d->pinned);
