@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--count", type=int, default=512, help="cfg3: problems in the batch")
     ap.add_argument("--fd", type=int, default=256, help="cfg4: finite-difference coordinates")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--host-pcg-loop", action="store_true",
+                    help="cfg0-cfg2: PCG steps launched from the host in chunks instead of the device-side "
+                         "graph loop (for profilers that do not follow conditional graph nodes)")
     return ap.parse_args()
 
 
@@ -350,7 +353,8 @@ def time_form(args, world, local, scene, precision, iterations):
     s_pin, i_pin = pinned_like(s_np, torch), pinned_like(i_np, torch)
     kw = dict(anchor=0, scale_view=1, iterations=iterations, shared_focal=True, huber=2.0, tolerance=1e-6,
               precision=precision)
-    ctl = tb.make_control(scene.C, scene.P, scene.M, **kw)
+    ctl = tb.make_control(scene.C, scene.P, scene.M, **kw,
+                          flags=_lib.TBA_FLAG_HOST_PCG_LOOP if args.host_pcg_loop else 0)
     ctl_timed = tb.make_control(scene.C, scene.P, scene.M, **kw, flags=_lib.TBA_FLAG_TIME_PRODUCTS)
     out = torch.empty(12 * scene.C + 3 * scene.P + 27, dtype=torch.float64, pin_memory=True).numpy()
     dev = tb.ShadeDevice.open(local)
@@ -468,7 +472,8 @@ def run_single(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": 1000 * summ["t_max"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
         "data": "synthetic (seeded; typecv_b200/synthetic.py)",
-        "config": {**workload(scene, args.config, iterations), "precision": head, "parallelism": f"replicas x{world}"},
+        "config": {**workload(scene, args.config, iterations), "precision": head, "parallelism": f"replicas x{world}",
+                   "pcg_loop": "host chunks" if args.host_pcg_loop else "device graph (conditional while node)"},
         "pcg_iterations_per_s": summ["pcg_iterations_per_s"],
         "final_cost": summ["final_cost"], "final_rmse_px": summ["final_rmse_px"],
         "e2e": {"value": summ["e2e"], "unit": UNIT, "h2d_bytes_per_step": int(reports[-1]["h2d_bytes"]),

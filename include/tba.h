@@ -65,6 +65,10 @@ typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
  * the poses, points and pixels), and report their difference in tba_report.product_error_* (for
  * the mixed form: the FP32 product's error).  Diagnostics only: two more products per call. */
 #define TBA_FLAG_PRODUCT_ERROR 2u
+/* TBA_FLAG_HOST_PCG_LOOP: launch the PCG steps from the host in chunks, as with
+ * TBA_FLAG_TIME_PRODUCTS but without the events, instead of the device-side graph loop (for
+ * profilers and tools that do not follow the kernels of conditional graph nodes).  Same results. */
+#define TBA_FLAG_HOST_PCG_LOOP 4u
 
 /*
  * The control block of one solve: the reference's `control` uniform

@@ -312,7 +312,8 @@ def test_mixed_precision_through_the_operator(device):
 def test_device_pcg_loop_matches_the_host_chunked_loop(device, precision):
     # Each PCG run is one launch of a CUDA graph whose while node repeats the PCG step until the PCG
     # stops or its budget is spent; with product timing on, the host issues the same steps in
-    # guarded chunks instead.  Both run the same kernels in the same order; the products' camera sums
+    # guarded chunks instead (also on request, without the events).  Both run the same kernels in the
+    # same order; the products' camera sums
     # are atomic adds, whose order varies from run to run, so the results agree to the rounding that
     # a PCG stopped at its tolerance carries through the LM iterations.  A second solve with the same
     # launch parameters launches the graph built by the first.
@@ -327,8 +328,11 @@ def test_device_pcg_loop_matches_the_host_chunked_loop(device, precision):
                                                               flags=_lib.TBA_FLAG_TIME_PRODUCTS, **kw), s, i)
         graph, rg = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, **kw), s, i)
         again, ra = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M, **kw), s, i)
+        host, rh = tb.solve_packed(device, tb.make_control(scene.C, scene.P, scene.M,
+                                                           flags=_lib.TBA_FLAG_HOST_PCG_LOOP, **kw), s, i)
         assert rc["product_launches"] > 0 and rg["product_launches"] == 0 and ra["product_launches"] == 0
-        for out, rep in ((graph, rg), (again, ra)):
+        assert rh["product_launches"] == 0
+        for out, rep in ((graph, rg), (again, ra), (host, rh)):
             assert abs(out[base + 6] - chunked[base + 6]) <= cost_rel * chunked[base + 6]
             assert np.max(np.abs(out[:12 * scene.C] - chunked[:12 * scene.C])) < pose_abs
             assert rep["lm_iterations"] == rc["lm_iterations"]

@@ -15,6 +15,7 @@ TBA_OK, TBA_ERROR_ARGUMENT, TBA_ERROR_BUDGET, TBA_ERROR_CUDA, TBA_ERROR_INTERNAL
 TBA_PRECISION_FP64, TBA_PRECISION_MIXED = 0, 1
 TBA_FLAG_TIME_PRODUCTS = 1
 TBA_FLAG_PRODUCT_ERROR = 2
+TBA_FLAG_HOST_PCG_LOOP = 4
 TBA_VJP_FLAG_TIME_PRODUCTS = 1
 TBA_WAIT_LIMIT_DEFAULT = 4194304
 

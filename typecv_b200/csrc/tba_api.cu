@@ -123,7 +123,8 @@ void check_control(const tba_control* c) {
       c->max_cg < 1 || c->max_cg > 256 ||
       !(std::isfinite(c->cg_tolerance) && c->cg_tolerance >= 1e-12 && c->cg_tolerance <= 1e-2) ||
       !(std::isfinite(c->stall_tolerance) && c->stall_tolerance >= 0 && c->stall_tolerance < 1) ||
-      c->precision > 1)
+      c->precision > 1 ||
+      (c->flags & ~(TBA_FLAG_TIME_PRODUCTS | TBA_FLAG_PRODUCT_ERROR | TBA_FLAG_HOST_PCG_LOOP)) != 0)
     argument("Invalid GPU BA scene/options");
   if (c->anchor >= c->cameras || c->scale_view >= c->cameras || c->anchor == c->scale_view)
     argument("Invalid GPU BA gauge cameras");
@@ -694,6 +695,7 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
   std::vector<std::pair<size_t, size_t>> product_events;
   std::vector<std::pair<size_t, uint32_t>> product_spans;  // (first event pair, real steps) per LM iteration
   const bool time_products = (ctl->flags & TBA_FLAG_TIME_PRODUCTS) != 0;
+  const bool host_loop = time_products || (ctl->flags & TBA_FLAG_HOST_PCG_LOOP) != 0;
   // Kernels per step of the device-side PCG loop launched last, while its step count is unread.
   uint32_t loop_kernels = 0;
   tba::launch_initialize(p, s);
@@ -742,15 +744,16 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
       product_error_max = bmax > 0 ? dmax / bmax : dmax;
       product_error_norm = b2 > 0 ? std::sqrt(d2 / b2) : std::sqrt(d2);
     }
-    // PCG runs.  Untimed, a run is one launch of the form's device-side PCG loop, which ends on the
+    // PCG runs.  By default a run is one launch of the form's device-side PCG loop, which ends on the
     // device; its step count is taken from the next state read (every run is followed by one in the
-    // same LM iteration).  Timed, the steps run in chunks of guarded iterations with events around
-    // each product; the read after each chunk only ends the loop early.
+    // same LM iteration).  With the host loop (timed products, or on request) the steps run in
+    // chunks of guarded iterations, events around each product when timed; the read after each
+    // chunk only ends the loop early.
     uint32_t done = 0, steps_before = 0;
     // `q` selects the product: the engine's own (FP32 factors in the mixed form), or the FP64
     // product of the mixed form's tail.  Only the engine's own products are timed.
     auto run_pcg = [&](uint32_t budget, const tba::Params& q, bool timed) {
-      if (!time_products) {
+      if (!host_loop) {
         if (budget <= done) return;
         PcgLoop& loop = d->pcg_loops[&q == &p ? 0 : 1];
         CUDA_TRY(build_pcg_loop(loop, q, s));
