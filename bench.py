@@ -391,7 +391,8 @@ def time_resident(args, world, local, scene, precision, iterations):
     poses = pinned_like(np.ascontiguousarray(s_np[:12 * C]), torch)
     points = pinned_like(np.ascontiguousarray(s_np[12 * C:12 * C + 3 * P]), torch)
     ctl = tb.make_control(C, P, scene.M, anchor=0, scale_view=1, iterations=iterations, shared_focal=True,
-                          huber=2.0, tolerance=1e-6, precision=precision)
+                          huber=2.0, tolerance=1e-6, precision=precision,
+                          flags=_lib.TBA_FLAG_HOST_PCG_LOOP if args.host_pcg_loop else 0)
     dev = tb.ShadeDevice.open(local)
     try:
         with ResidentScene(dev, ctl, s_np, i_np) as rs:

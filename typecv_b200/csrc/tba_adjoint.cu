@@ -547,22 +547,25 @@ __global__ void __launch_bounds__(kAdjProductThreads) k_adj_product(AdjParams A)
   }
 }
 
-// S p = U_c p_c + the blocks' partial rows: 32 rows per block, each of its 8 warps summing every
-// 8th block's partial rows (coalesced), then the 8 sums in a fixed order.
-__global__ void __launch_bounds__(256) k_adj_columns(AdjParams A) {
-  __shared__ double part[8][33];
+// S p = U_c p_c + the blocks' partial rows: 32 rows per block, each of its kAdjColumnWarps warps
+// summing every kAdjColumnWarps-th block's partial rows (coalesced; short dependent chains, about
+// nine loads a lane at 296 product blocks), then the warps' sums in a fixed order.
+constexpr int kAdjColumnWarps = 32;
+
+__global__ void __launch_bounds__(32 * kAdjColumnWarps) k_adj_columns(AdjParams A) {
+  __shared__ double part[kAdjColumnWarps][33];
   if (A.state[A_ACTIVE] == 0) return;
   const uint32_t n = 6 * A.C;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t j = blockIdx.x * 32 + lane;
   double s = 0;
   if (j < n)
-    for (uint32_t b = warp; b < A.prod_blocks; b += 8) s += A.part[size_t(b) * n + j];
+    for (uint32_t b = warp; b < A.prod_blocks; b += kAdjColumnWarps) s += A.part[size_t(b) * n + j];
   part[warp][lane] = s;
   __syncthreads();
   if (warp != 0 || j >= n) return;
   double sum = 0;
-  for (int w = 0; w < 8; w++) sum += part[w][lane];
+  for (int w = 0; w < kAdjColumnWarps; w++) sum += part[w][lane];
   const uint32_t c = j / 6, a = j % 6;
   const double* U = A.U + 21 * size_t(c);
   const double* pc = A.p + 6 * size_t(c);
@@ -919,7 +922,7 @@ uint32_t adj_launch_pcg_step(const AdjParams& a, cudaStream_t s, cudaEvent_t bef
     if (before) cudaEventRecord(before, s);
     k_adj_product<<<a.prod_blocks, kAdjProductThreads, adj_product_smem(a.C), s>>>(a);
     if (after) cudaEventRecord(after, s);
-    k_adj_columns<<<(6 * a.C + 31) / 32, 256, 0, s>>>(a);
+    k_adj_columns<<<(6 * a.C + 31) / 32, 32 * kAdjColumnWarps, 0, s>>>(a);
   } else {
     k_adj_prod_points<<<grid_for(a.P, 256), 256, 0, s>>>(a);
     k_adj_prod_cameras<<<a.C, 128, 0, s>>>(a);
