@@ -58,7 +58,8 @@ typedef enum { TBA_PRECISION_FP64 = 0, TBA_PRECISION_MIXED = 1 } tba_precision;
 /* TBA_FLAG_TIME_PRODUCTS: bracket every Schur product with CUDA events and report their total
  * device time in tba_report.product_ms (a few microseconds of host work per PCG iteration).
  * Without it each PCG run is one launch of a CUDA graph that repeats the PCG step on the device
- * until the PCG stops; with it the host launches the steps in chunks, with the same results. */
+ * until the PCG stops (or, where the driver cannot build conditional graph nodes, from the host);
+ * with it the host launches the steps in chunks, with the same results. */
 #define TBA_FLAG_TIME_PRODUCTS 1u
 /* TBA_FLAG_PRODUCT_ERROR: once, on the first PCG direction of the first LM iteration, evaluate S p
  * with the solve's own Schur product and with the FP64 two-pass product (Jacobians recomputed from

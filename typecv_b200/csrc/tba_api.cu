@@ -72,6 +72,8 @@ struct tba_device {
   // tail) and the adjoint's.
   PcgLoop pcg_loops[2];
   PcgLoop adj_loop;
+  // Set when the driver could not build a conditional graph: the PCG steps then run from the host.
+  bool host_pcg_only = false;
 };
 
 // A scene resident on the device between calls: the packed arrays of one problem and its host
@@ -419,6 +421,20 @@ cudaError_t build_adjoint_loop(PcgLoop& loop, const tba::AdjParams& a, cudaStrea
   });
 }
 
+// Whether a device-side loop was built.  A driver that cannot build conditional graph nodes makes
+// the handle run every later PCG from the host (the same kernels, launched in chunks); any other
+// failure is the call's error.
+bool device_loop_ready(tba_device* d, PcgLoop& loop, cudaError_t built) {
+  if (built == cudaSuccess) return true;
+  loop.release();
+  if (built == cudaErrorNotSupported || built == cudaErrorStreamCaptureUnsupported) {
+    cudaGetLastError();
+    d->host_pcg_only = true;
+    return false;
+  }
+  throw Fail{TBA_ERROR_CUDA, std::string("device PCG loop: ") + cudaGetErrorString(built)};
+}
+
 cudaEvent_t event(tba_device* d, size_t k) {
   while (d->events.size() <= k) {
     cudaEvent_t e;
@@ -753,15 +769,16 @@ void solve(tba_device* d, const tba_control* ctl, const double* scene, const uin
     // `q` selects the product: the engine's own (FP32 factors in the mixed form), or the FP64
     // product of the mixed form's tail.  Only the engine's own products are timed.
     auto run_pcg = [&](uint32_t budget, const tba::Params& q, bool timed) {
-      if (!host_loop) {
+      if (!host_loop && !d->host_pcg_only) {
         if (budget <= done) return;
         PcgLoop& loop = d->pcg_loops[&q == &p ? 0 : 1];
-        CUDA_TRY(build_pcg_loop(loop, q, s));
-        tba::launch_pcg_loop_begin(q, budget - done, s);
-        launches++;
-        CUDA_TRY(cudaGraphLaunch(loop.exec, s));
-        loop_kernels = loop.body_kernels;
-        return;
+        if (device_loop_ready(d, loop, build_pcg_loop(loop, q, s))) {
+          tba::launch_pcg_loop_begin(q, budget - done, s);
+          launches++;
+          CUDA_TRY(cudaGraphLaunch(loop.exec, s));
+          loop_kernels = loop.body_kernels;
+          return;
+        }
       }
       const size_t first_pair = product_events.size();
       uint32_t chunk = 8;
@@ -1398,10 +1415,10 @@ void solve_vjp(tba_device* d, const tba_vjp_control* vc, const double* scene, co
     CUDA_TRY(cudaGetLastError());
     uint32_t done = 0;
     const bool timed = time_products && A.prod_blocks;
-    const bool on_device = !timed && vc->max_cg > 0;
+    const bool on_device = !timed && vc->max_cg > 0 && !d->host_pcg_only &&
+                           device_loop_ready(d, d->adj_loop, build_adjoint_loop(d->adj_loop, A, s));
     if (on_device) {
       // One launch of the device-side PCG loop, which stops on the device.
-      CUDA_TRY(build_adjoint_loop(d->adj_loop, A, s));
       launches += tba::adj_launch_loop_begin(A, vc->max_cg, s);
       CUDA_TRY(cudaGraphLaunch(d->adj_loop.exec, s));
       done = vc->max_cg;
