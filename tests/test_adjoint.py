@@ -78,6 +78,22 @@ def test_vjp_matches_the_dense_reference(device):
     assert np.all(np.abs(kbar - kbar_d) <= 1e-6 * np.abs(kbar_d) + 1e-12)
 
 
+def test_vjp_device_loop_matches_the_host_loop(device):
+    # Each linear solve's PCG is one launch of a graph with a conditional while node; timing the
+    # products runs the same steps from the host in chunks.  The product's camera sums are atomic
+    # adds, so the two agree to the PCG's tolerance, not bit for bit.
+    sc = S.helix_scene(seed=22, cameras=10, points=500)
+    s, i = converged(device, sc)
+    g = unit_cotangent(12 * sc.C + 3 * sc.P, 5)
+    yd, kd, _, rd = AD.bundle_vjp(device, sc.C, sc.P, sc.M, s, i, g, newton_steps=4)
+    yh, kh, _, rh = AD.bundle_vjp(device, sc.C, sc.P, sc.M, s, i, g, newton_steps=4, time_products=True)
+    assert rd["failed"] == 0 and rh["failed"] == 0
+    assert rd["product_launches"] == 0 and rh["product_launches"] > 0
+    assert np.linalg.norm(yd - yh) <= 1e-8 * np.linalg.norm(yh)
+    assert np.all(np.abs(kd - kh) <= 1e-8 * np.abs(kh) + 1e-12)
+    assert abs(rd["cg_iterations"] - rh["cg_iterations"]) <= max(4, 0.05 * rh["cg_iterations"])
+
+
 def test_baseline_cotangent_has_no_product(device):
     # The solver keeps the anchor-to-scale-camera baseline, so no pixel moves it.
     sc = S.helix_scene(seed=23, cameras=12, points=800)
