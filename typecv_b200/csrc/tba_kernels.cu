@@ -620,8 +620,9 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // after the camera sums, so the per-observation read of it is an on-chip gather; one block of
 // kStagedThreads per SM.  With FP32 factors the kernel fits 64 registers and takes 1,024 threads
 // (32 warps to cover the latency of the loads each lane issues before its arithmetic): 0.157 ->
-// 0.137 ms for 1,500 cameras / 6.18M observations.  The FP64 kernel needs 80 and stays at 768
-// (at 1,024 it spills and the busier L1 data pipe makes it slower, 0.196 -> 0.204 ms).
+// 0.137 ms for 1,500 cameras / 6.18M observations.  The FP64 kernel, which loads V_p^-1 in the last
+// lane of each point only and reads the direction as pairs, fits 64 registers too (4-8 bytes
+// spilled) and also takes 1,024 threads: 0.197 -> 0.188 ms against 768.
 // Otherwise it is read from global memory, two blocks of kProductThreads.
 // Both shared arrays are component-major (the sums: value j of camera c at j * C + c; the direction:
 // pair k of camera c at k * C + c, read as one 16- or 8-byte word): the lanes of a warp touch random
