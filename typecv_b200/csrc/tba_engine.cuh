@@ -60,7 +60,9 @@ enum StateWord : int {
 constexpr int kTaskObs = 32;        // observations per warp task (one per lane)
 constexpr int kFactors = 12;        // stored Jacobian factors per observation
 constexpr int kProductThreads = 384;  // two blocks per SM
-constexpr int kStagedThreads = 1024;  // one block per SM, direction staged in shared memory (FP64 factors)
+constexpr int kStagedThreads = 768;   // one block per SM, direction staged in shared memory (FP64 factors)
+constexpr int kStagedThreadsWide = 1024;  // the same on large problems (64 registers, a few bytes spilled)
+constexpr uint32_t kWideObservations = 2000000;  // observations from which the FP64 product takes 1,024 threads
 constexpr int kStagedThreadsF32 = 1024;  // the same with FP32 factors (64 registers a thread)
 constexpr int kStagedSmemLimit = 227 * 1024 - 64;  // the dynamic share; the rest is static
 // Bytes of a product block's camera sums (6C values of `word` bytes), rounded to 16.

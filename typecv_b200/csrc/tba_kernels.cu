@@ -620,9 +620,10 @@ __global__ void __launch_bounds__(kCameraThreads, TBA_CAMERA_MIN_BLOCKS) k_schur
 // after the camera sums, so the per-observation read of it is an on-chip gather; one block of
 // kStagedThreads per SM.  With FP32 factors the kernel fits 64 registers and takes 1,024 threads
 // (32 warps to cover the latency of the loads each lane issues before its arithmetic): 0.157 ->
-// 0.137 ms for 1,500 cameras / 6.18M observations.  The FP64 kernel, which loads V_p^-1 in the last
-// lane of each point only and reads the direction as pairs, fits 64 registers too (4-8 bytes
-// spilled) and also takes 1,024 threads: 0.197 -> 0.188 ms against 768.
+// 0.137 ms for 1,500 cameras / 6.18M observations.  The FP64 kernel runs 768 threads at 80
+// registers; from kWideObservations observations (WIDE) it is compiled for 1,024 threads at 64
+// registers (4-8 bytes spilled): 0.197 -> 0.188 ms at 6.18M observations, while at 0.75M (under
+// six tasks a warp) the extra warps cost more in the block's tail than they hide (1-5% slower).
 // Otherwise it is read from global memory, two blocks of kProductThreads.
 // Both shared arrays are component-major (the sums: value j of camera c at j * C + c; the direction:
 // pair k of camera c at k * C + c, read as one 16- or 8-byte word): the lanes of a warp touch random
@@ -717,8 +718,9 @@ __device__ inline void factor_wt_t(const Factors<T>& f, const T (&xw)[6], T xf, 
   for (int k = 0; k < 3; k++) t[k] = au * f.ju[k] + av * f.jv[k];
 }
 
-template <bool SHARED, typename T, typename A, bool STAGED>
-__global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 : kStagedThreads) : kProductThreads,
+template <bool SHARED, typename T, typename A, bool STAGED, bool WIDE = false>
+__global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 : (WIDE ? kStagedThreadsWide : kStagedThreads))
+                                         : kProductThreads,
                                   STAGED ? 1 : 2) k_product_f(Params P) {
   extern __shared__ double4 product_smem[];
   __shared__ double focal_acc;
@@ -1569,8 +1571,12 @@ size_t product_smem_bytes(const Params& p) {
   return product_sums_bytes(p.C, product_sum_word(p)) + (product_staged(p) ? 6 * size_t(p.C) * word : 0);
 }
 
+// The FP64 staged product takes 1,024 threads on large problems (enough tasks a warp).
+bool product_wide(const Params& p) { return !p.F32 && product_staged(p) && p.M >= kWideObservations; }
+
 int product_threads(const Params& p) {
-  return product_staged(p) ? (p.F32 ? kStagedThreadsF32 : kStagedThreads) : kProductThreads;
+  if (!product_staged(p)) return kProductThreads;
+  return p.F32 ? kStagedThreadsF32 : (product_wide(p) ? kStagedThreadsWide : kStagedThreads);
 }
 
 namespace {
@@ -1579,9 +1585,11 @@ namespace {
 template <bool SHARED>
 const void* product_kernel_of(const Params& p) {
   const bool st = product_staged(p);
-  if (!p.F32)
+  if (!p.F32) {
+    if (product_wide(p)) return reinterpret_cast<const void*>(k_product_f<SHARED, double, double, true, true>);
     return st ? reinterpret_cast<const void*>(k_product_f<SHARED, double, double, true>)
               : reinterpret_cast<const void*>(k_product_f<SHARED, double, double, false>);
+  }
   return st ? reinterpret_cast<const void*>(k_product_f<SHARED, float, float, true>)
             : reinterpret_cast<const void*>(k_product_f<SHARED, float, float, false>);
 }
@@ -1597,6 +1605,8 @@ cudaError_t configure_kernels() {
       reinterpret_cast<const void*>(k_product_f<true, double, double, false>),
       reinterpret_cast<const void*>(k_product_f<false, double, double, true>),
       reinterpret_cast<const void*>(k_product_f<true, double, double, true>),
+      reinterpret_cast<const void*>(k_product_f<false, double, double, true, true>),
+      reinterpret_cast<const void*>(k_product_f<true, double, double, true, true>),
       reinterpret_cast<const void*>(k_product_f<false, float, float, false>),
       reinterpret_cast<const void*>(k_product_f<true, float, float, false>),
       reinterpret_cast<const void*>(k_product_f<false, float, float, true>),
