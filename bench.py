@@ -87,15 +87,15 @@ def workload(scene, config, iterations):
 
 def product_bytes(scene, shared, prod_blocks, factor_bytes=8):
     """Algorithmic DRAM bytes of one launch of the one-pass Schur product k_product_f: per
-    observation its 12 stored Jacobian factors (8 B each in FP64, 4 B in the mixed form), its point
-    index and its camera-order schedule word (8 B); per point V_p^-1 (6 values of the factors' size:
-    the mixed form reads an FP32 copy); per warp task its first observation (4 B, about one task per
-    28 observations, counted per point here); the direction in world axes (6C words) and the
-    per-block partial rows (prod_blocks x m words, written by the product and read by the column
-    reduction)."""
+    observation its 12 stored Jacobian factors (8 B each in FP64, 4 B in the mixed form) and its
+    camera and point indices (8 B); per point V_p^-1 (6 values of the factors' size: the mixed form
+    reads an FP32 copy); per warp task its first observation (4 B, about one task per 28
+    observations, counted per point here); the direction in world axes (6C FP64 words) and the
+    per-block partial rows (prod_blocks x m values of the factors' size, written by the product and
+    read by the column reduction)."""
     m = 6 * scene.C + (1 if shared else 0)
     return (scene.M * (12 * factor_bytes + 8) + scene.P * (6 * factor_bytes + 4) + 8 * 6 * scene.C
-            + 2 * 8 * m * prod_blocks)
+            + 2 * factor_bytes * m * prod_blocks)
 
 
 def two_pass_bytes(scene, shared):

@@ -865,43 +865,60 @@ __global__ void __launch_bounds__(STAGED ? (sizeof(T) == 4 ? kStagedThreadsF32 :
     if (lane == 0) atomicAdd(&focal_acc, -ef);
   }
   __syncthreads();
-  // Rotate each camera's sums into its axes and write this block's partial row.
-  double* out = P.acc_part + size_t(blockIdx.x) * m;
-  for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) {
-    double a[6];
-    for (int j = 0; j < 6; j++) a[j] = double(acc[j * C + c]);
-    const double* R = P.poses + 12 * size_t(c);
-    for (int r = 0; r < 3; r++) {
-      out[6 * c + r] = R[3 * r] * a[0] + R[3 * r + 1] * a[1] + R[3 * r + 2] * a[2];
-      out[6 * c + 3 + r] = R[3 * r] * a[3] + R[3 * r + 1] * a[4] + R[3 * r + 2] * a[5];
-    }
+  // This block's partial row: each camera's sums in world axes and in A (the column sums add the
+  // blocks' rows in FP64 and rotate each camera's total into its axes once).
+  A* out = reinterpret_cast<A*>(P.acc_part) + size_t(blockIdx.x) * m;
+  for (uint32_t j = threadIdx.x; j < 6 * C; j += blockDim.x) out[j] = acc[(j % 6) * C + j / 6];
+  if (SHARED && threadIdx.x == 0) out[m - 1] = A(focal_acc);
+}
+
+// Column j of the one-pass product's partial rows summed over the blocks in a fixed order (world
+// axes for a camera row), from FP32 rows when the product ran on FP32 factors.
+__device__ inline double partial_column(const Params& P, bool f32, uint32_t j, uint32_t first, uint32_t step) {
+  double s = 0;
+  if (f32) {
+    const float* rows = reinterpret_cast<const float*>(P.acc_part);
+    for (uint32_t g = first; g < P.prod_blocks; g += step) s += double(__ldcg(rows + size_t(g) * P.m + j));
+  } else {
+    for (uint32_t g = first; g < P.prod_blocks; g += step) s += __ldcg(P.acc_part + size_t(g) * P.m + j);
   }
-  if (SHARED && threadIdx.x == 0) out[m - 1] = focal_acc;
+  return s;
+}
+
+// Row r (0..5) of camera c's world-axis sums w6 turned into the camera's axes: R w for the rotation
+// rows (0..2), R w for the translation rows (3..5).
+__device__ inline double camera_axis_row(const double* R, const double* w6, uint32_t r) {
+  const uint32_t i = r % 3, b = r < 3 ? 0 : 3;
+  return R[3 * i] * w6[b] + R[3 * i + 1] * w6[b + 1] + R[3 * i + 2] * w6[b + 2];
 }
 
 // The column sums of the one-pass product's partial rows (fixed order), then the camera rows of
 // S p = U_c p_c + H_cf p_f + sum, their p . Sp share; the last block adds the focal row and forms
 // alpha (the reference's breakdown checks).
+constexpr uint32_t kColumnRows = 30;  // rows of a column block: five whole cameras
+
 template <bool SHARED>
 __global__ void __launch_bounds__(256) k_product_columns(Params P) {
   __shared__ double part[8][33];
+  __shared__ double world[32];
   __shared__ double red[2 * 8];
   if (P.state[S_CG_ACTIVE] == 0) return;
   const uint32_t n = 6 * P.C, m = P.m;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t j = blockIdx.x * 32 + lane;
-  double s = 0;
-  if (j < m)
-    for (uint32_t g = warp; g < P.prod_blocks; g += 8) s += P.acc_part[size_t(g) * m + j];
-  part[warp][lane] = s;
+  const uint32_t j = blockIdx.x * kColumnRows + lane;
+  const bool row = uint32_t(lane) < kColumnRows && j < m;
+  part[warp][lane] = row ? partial_column(P, P.F32 != nullptr, j, warp, 8) : 0.0;
   __syncthreads();
   double v[2] = {0, 0};
   if (warp == 0) {
     double sum = 0;
 #pragma unroll
     for (int w = 0; w < 8; w++) sum += part[w][lane];
-    if (j < n) {
+    world[lane] = sum;
+    __syncwarp();
+    if (row && j < n) {
       const uint32_t c = j / 6, r = j % 6;
+      sum = camera_axis_row(P.poses + 12 * size_t(c), world + 6 * (uint32_t(lane) / 6), r);
       const double* U = P.camU + 21 * size_t(c);
       const double* pc = P.p + 6 * size_t(c);
       double up = 0;
@@ -914,7 +931,7 @@ __global__ void __launch_bounds__(256) k_product_columns(Params P) {
       }
       P.Sp[j] = sp;
       v[0] = P.p[j] * sp;
-    } else if (SHARED && j == n) {
+    } else if (SHARED && row && j == n) {
       P.Sp[n] = sum;
     }
   }
@@ -1110,8 +1127,13 @@ __global__ void __launch_bounds__(256) k_product_rows(Params P, int onepass, dou
     const uint32_t c = j / 6, r = j % 6;
     double sum = 0;
     if (onepass) {
-      if (P.active[c] != 0)
-        for (uint32_t b = 0; b < P.prod_blocks; b++) sum += P.acc_part[size_t(b) * P.m + j];
+      if (P.active[c] != 0) {
+        // The world-axis sums of this row's triple, rotated into the camera's axes.
+        double w6[6] = {0, 0, 0, 0, 0, 0};
+        const uint32_t base = r < 3 ? 0 : 3;
+        for (uint32_t k = 0; k < 3; k++) w6[base + k] = partial_column(P, P.F32 != nullptr, 6 * c + base + k, 0, 1);
+        sum = camera_axis_row(P.poses + 12 * size_t(c), w6, r);
+      }
     } else {
       for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum -= P.chunk_prod[8 * size_t(ch) + r];
     }
@@ -1125,7 +1147,7 @@ __global__ void __launch_bounds__(256) k_product_rows(Params P, int onepass, dou
     double sp = P.state[S_FOCAL_DIAG] * P.p[n];
     for (uint32_t k = 0; k < n; k++) sp += P.camHcf[k] * P.p[k];
     if (onepass)
-      for (uint32_t b = 0; b < P.prod_blocks; b++) sp += P.acc_part[size_t(b) * P.m + n];
+      sp += partial_column(P, P.F32 != nullptr, n, 0, 1);
     else
       for (uint32_t ch = 0; ch < P.nchunks; ch++) sp -= P.chunk_prod[8 * size_t(ch) + 6];
     out[n] = sp;
@@ -1175,12 +1197,18 @@ __global__ void k_refine_direction(Params P) {
 
 __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
   __shared__ double rs[kUpdateRows];
+  __shared__ double ws[kUpdateRows];
   __shared__ double red[4 * (kUpdateThreads / 32)];
   double* st = P.state;
   if (st[S_REFINE] == 0) return;
   const uint32_t n = 6 * P.C;
   const uint32_t row = blockIdx.x * kUpdateRows + threadIdx.x;
   const bool mine = threadIdx.x < uint32_t(kUpdateRows) && row < n;
+  const bool onepass = P.factored && P.F;
+  // The one-pass product (over the FP64 factors) left world-axis FP64 partial rows; a block's rows
+  // are whole cameras, so each camera's column sums meet in shared memory to be rotated.
+  if (onepass && threadIdx.x < uint32_t(kUpdateRows)) ws[threadIdx.x] = mine ? partial_column(P, false, row, 0, 1) : 0.0;
+  __syncthreads();
   double rr = 0;
   double v[4] = {0, 0, 0, 0};  // r.r, r.z (camera rows), H_cf . x, observation share of the focal row
   if (mine) {
@@ -1188,9 +1216,9 @@ __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
     // sum_i W_i y_p of the camera: the column sum of the one-pass product's partial rows (which hold
     // its negative; a fixed camera's rows are discarded), or the two-pass product's chunk sums.
     double sum = 0;
-    if (P.factored && P.F) {
+    if (onepass) {
       if (P.active[c] != 0)
-        for (uint32_t b = 0; b < P.prod_blocks; b++) sum -= P.acc_part[size_t(b) * P.m + row];
+        sum = -camera_axis_row(P.poses + 12 * size_t(c), ws + (threadIdx.x - j), j);
     } else {
       for (uint32_t ch = P.cam_chunk[c]; ch < P.cam_chunk[c + 1]; ch++) sum += P.chunk_prod[8 * size_t(ch) + j];
     }
@@ -1208,7 +1236,7 @@ __global__ void __launch_bounds__(kUpdateThreads) k_refine(Params P) {
     rs[threadIdx.x] = rr;
   }
   if (P.shared) {
-    if (P.factored && P.F)
+    if (onepass)
       for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < P.prod_blocks; b += gridDim.x * blockDim.x)
         v[3] -= P.acc_part[size_t(b) * P.m + (P.m - 1)];
     else
@@ -1548,7 +1576,7 @@ __global__ void k_pack(Params P) {
 
 uint32_t product_finish_blocks(const Params& p) {
   const uint32_t a = (6 * p.C + kReduceThreads - 1) / kReduceThreads, b = (p.m + kUpdateRows - 1) / kUpdateRows;
-  const uint32_t c = (p.m + 31) / 32;
+  const uint32_t c = (p.m + kColumnRows - 1) / kColumnRows;
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
@@ -1660,8 +1688,8 @@ void launch_product(const Params& p, cudaStream_t s) {
 }
 void launch_product_finish(const Params& p, cudaStream_t s) {
   if (p.factored) {
-    if (p.shared) k_product_columns<true><<<(p.m + 31) / 32, 256, 0, s>>>(p);
-    else k_product_columns<false><<<(p.m + 31) / 32, 256, 0, s>>>(p);
+    if (p.shared) k_product_columns<true><<<(p.m + kColumnRows - 1) / kColumnRows, 256, 0, s>>>(p);
+    else k_product_columns<false><<<(p.m + kColumnRows - 1) / kColumnRows, 256, 0, s>>>(p);
   } else {
     const uint32_t rb = (6 * p.C + kReduceThreads - 1) / kReduceThreads;
     if (p.shared) k_product_reduce<true><<<rb, kReduceThreads, 0, s>>>(p);
