@@ -119,7 +119,8 @@ struct Params {
   uint32_t prod_blocks;  // grid of the one-pass product
   double* pw;          // 6C: the PCG direction of each camera in world axes (R^T omega, R^T v)
   double* xw;          // 6C: the PCG solution of each camera in world axes
-  double* acc_part;    // prod_blocks x m: per-block camera sums of the one-pass product
+  double* acc_part;    // prod_blocks x m: per-block camera sums of the one-pass product, in world axes
+                       // and in the block sums' type (FP32 values for the FP32 product)
   double* camU;     // 21C
   double* camMinv;  // 36C
   double* camRhs;   // 6C
