@@ -1118,9 +1118,9 @@ __global__ void k_pcg_direction(Params P) {
 
 // ---- Diagnostics: S p of one product, every row, into `out` --------------------------------------
 //
-// `onepass`: from the one-pass product's partial rows (which hold -sum_i W_i y_p in world axes), else from the
-// two-pass product's chunk sums (+sum_i W_i y_p); then U_c p_c, the focal couplings and the focal
-// row, as k_product_columns and k_product_reduce form them.  Writes no state.
+// `onepass`: from the one-pass product's partial rows (which hold -sum_i W_i y_p in world axes),
+// else from the two-pass product's chunk sums (+sum_i W_i y_p); then U_c p_c, the focal couplings
+// and the focal row, as k_product_columns and k_product_reduce form them.  Writes no state.
 __global__ void __launch_bounds__(256) k_product_rows(Params P, int onepass, double* out) {
   const uint32_t n = 6 * P.C, j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n) {
